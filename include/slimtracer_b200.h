@@ -1,0 +1,335 @@
+/*
+ * slimtracer_b200.h -- C ABI of the B200 (sm_100a) per-pixel trace path.
+ *
+ * Drop-in for the GPU seam of SlimTracin's renderer: the reference compiles
+ * renderer/renderer_GPU.h into the app when built with nvcc
+ * (renderer/renderer.h:7-17) and calls its hooks from
+ * RayTracingRenderer's constructor and render() (renderer/renderer.h:60,
+ * 69-81).  This library exports the same hooks as plain C functions taking
+ * pointers to POD mirrors of the reference's structs, laid out byte for
+ * byte like the reference's own types on LP64 with 4-byte u32
+ * (static-asserted below), so an app passes `(const SlimSceneData*)&scene`.
+ *
+ * Differences from the reference's hooks, all deliberate:
+ *   - every call returns an int status (SLIM_OK == 0) instead of printing
+ *     and exit()ing (core/base.h:17-27) or silently ignoring errors in
+ *     release builds (core/base.h:46); slimGetLastError() describes it;
+ *   - the library never falls back to a CPU path: without a usable CUDA
+ *     device every call fails with SLIM_ERR_CUDA.
+ */
+#ifndef SLIMTRACER_B200_H
+#define SLIMTRACER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SLIM_OK              0
+#define SLIM_ERR_ARGUMENT    1   /* null pointer, bad count or size          */
+#define SLIM_ERR_CUDA        2   /* CUDA runtime error (no device, OOM, ...) */
+#define SLIM_ERR_STATE       3   /* call order (e.g. render before init)     */
+#define SLIM_ERR_LIMIT       4   /* a fixed capacity would be exceeded       */
+#define SLIM_ERR_IO          5   /* file missing, truncated or malformed     */
+#define SLIM_ERR_STACK       6   /* a traversal stack overflowed (device)    */
+
+/* ---- enums and flags (core/base.h:137-149,402-414,626-633,655-660) ----- */
+enum { SLIM_GEOMETRY_NONE = 0, SLIM_GEOMETRY_MESH, SLIM_GEOMETRY_GRID, SLIM_GEOMETRY_BOX,
+       SLIM_GEOMETRY_CURVE, SLIM_GEOMETRY_TET, SLIM_GEOMETRY_QUAD, SLIM_GEOMETRY_SPHERE,
+       SLIM_GEOMETRY_LIGHT };
+enum { SLIM_BRDF_LAMBERT = 0, SLIM_BRDF_BLINN, SLIM_BRDF_PHONG, SLIM_BRDF_COOK_TORRANCE };
+enum { SLIM_RENDER_NORMALS = 0, SLIM_RENDER_NORMAL_MAP, SLIM_RENDER_BEAUTY, SLIM_RENDER_DEPTH,
+       SLIM_RENDER_MIP_LEVEL, SLIM_RENDER_UVS };
+enum { SLIM_AA_NONE = 0, SLIM_AA_MSAA, SLIM_AA_SSAA };
+#define SLIM_MATERIAL_IS_REFLECTIVE   1u
+#define SLIM_MATERIAL_IS_REFRACTIVE   2u
+#define SLIM_MATERIAL_IS_EMISSIVE     4u
+#define SLIM_MATERIAL_HAS_ALBEDO_MAP 16u
+#define SLIM_MATERIAL_HAS_NORMAL_MAP 32u
+#define SLIM_GEOMETRY_IS_VISIBLE      1u
+#define SLIM_GEOMETRY_IS_SHADOWING    2u
+#define SLIM_GEOMETRY_IS_TRANSPARENT  4u
+#define SLIM_LIGHT_IS_DIRECTIONAL     1u   /* scene/material.h:10-15 */
+#define SLIM_LIGHT_IS_SHADOWING       2u
+#define SLIM_SCENE_HAD_EMISSIVE_QUADS 1u   /* scene/scene.h:27 */
+/* ImageInfo.flags bits (core/base.h:1264-1276) */
+#define SLIM_IMAGE_ALPHA    (1u << 0)
+#define SLIM_IMAGE_LINEAR   (1u << 1)
+#define SLIM_IMAGE_TILE     (1u << 2)
+#define SLIM_IMAGE_CHANNEL  (1u << 3)
+#define SLIM_IMAGE_MIPMAP   (1u << 4)
+#define SLIM_IMAGE_FLIP     (1u << 5)
+#define SLIM_IMAGE_WRAP     (1u << 6)
+#define SLIM_IMAGE_NORMAL   (1u << 7)
+#define SLIM_IMAGE_CUBEMAP  (1u << 8)
+
+/* ---- POD mirrors of the reference structs ------------------------------ */
+typedef struct { float x, y, z; } SlimVec3;                       /* math/vec3.h:5   */
+typedef struct { float x, y; } SlimVec2;                          /* math/vec2.h:255 */
+typedef struct { SlimVec3 min, max; } SlimAABB;                   /* math/vec3.h:423 */
+
+/* OrientationUsingQuaternion = quat{axis, amount} + Orientation's euler
+ * cache x,y,z (math/quat.h:3-6, core/base.h:546-622). */
+typedef struct { SlimVec3 axis; float amount; float euler[3]; } SlimOrientation;
+typedef struct { SlimOrientation orientation; SlimVec3 position, scale; } SlimTransform;   /* core/transform.h:5-8  */
+typedef struct {                                                                          /* core/transform.h:59-65 */
+    SlimTransform transform;
+    int32_t type;           /* SLIM_GEOMETRY_*                      */
+    uint32_t material_id;
+    uint32_t id;            /* mesh index for SLIM_GEOMETRY_MESH    */
+    uint8_t flags;          /* SLIM_GEOMETRY_IS_*                   */
+    uint8_t _pad[3];
+    int32_t color;          /* ColorID, unused by the tracer        */
+} SlimGeometry;
+typedef struct {                                                                          /* scene/material.h:93-110 */
+    float albedo[3];
+    float roughness;
+    uint8_t flags, texture_count, texture_ids[2];
+    int32_t brdf;
+    float normal_magnitude;
+    SlimVec2 uv_repeat;
+    float emission[3];
+    float IOR;
+    float reflectivity[3];
+    float metalness;
+} SlimMaterial;
+typedef struct {                                                                          /* scene/material.h:17-21 */
+    float color[3];
+    SlimVec3 position_or_direction;
+    float intensity;
+    uint8_t flags;
+    uint8_t _pad[3];
+} SlimLight;
+typedef struct {                                                                          /* scene/bvh.h:5-16 */
+    SlimAABB aabb;
+    uint32_t first_index;
+    uint16_t leaf_count;
+    uint8_t depth, flags;
+} SlimBVHNode;
+typedef struct { SlimBVHNode *nodes; uint32_t node_count; uint8_t height; uint8_t _pad[3]; } SlimBVH;  /* scene/bvh.h:18-21 */
+typedef struct {                                                                          /* scene/mesh.h:19-23 */
+    float local_to_tangent[9];   /* mat3 columns X, Y, Z */
+    SlimVec3 position, normal, n1, n2, n3;
+    SlimVec2 uv1, uv2, uv3;
+    float uv_coverage, padding;
+} SlimTriangle;
+typedef struct {                                                                          /* scene/mesh.h:25-41 */
+    SlimAABB aabb;
+    SlimBVH bvh;
+    SlimTriangle *triangles;
+    SlimVec3 *vertex_positions, *vertex_normals;
+    SlimVec2 *vertex_uvs;
+    uint32_t *vertex_position_indices, *vertex_normal_indices, *vertex_uvs_indices;  /* [triangle][3] */
+    uint32_t *edge_vertex_indices;                                                     /* [edge][2]     */
+    uint32_t triangle_count, vertex_count, edge_count, normals_count, uvs_count;
+    uint32_t _pad;
+} SlimMesh;
+typedef struct { uint8_t R[4], G[4], B[4]; } SlimTexelQuad;   /* {TL,TR,BL,BR} per channel, core/texture.h:5-11 */
+typedef struct { uint32_t width, height; SlimTexelQuad *texel_quads; } SlimTextureMip;   /* core/texture.h:13-15 */
+typedef struct {                                              /* ImageInfo + mips, core/base.h:1233-1284, core/texture.h:44-45 */
+    uint32_t width, height, size, stride, tile_width, tile_height;
+    uint32_t mip_count;
+    uint32_t flags;          /* SLIM_IMAGE_* */
+    SlimTextureMip *mips;
+} SlimTexture;
+typedef struct {                                              /* scene/scene.h:17-19 */
+    uint32_t geometries, cameras, lights, materials, textures, meshes, grids, boxes, tets, quads, curves;
+} SlimSceneCounts;
+typedef struct {                                              /* scene/scene.h:35-56 */
+    SlimSceneCounts counts;
+    uint16_t flags, mesh_stack_size;
+    SlimGeometry *geometries;
+    void *cameras;
+    SlimLight *lights;
+    SlimMaterial *materials;
+    SlimTexture *textures;
+    SlimMesh *meshes;
+    void *grids, *boxes, *tets, *quads, *curves;
+    SlimAABB *aabbs;
+    void *io, *bvh_builder;
+    uint32_t *bvh_leaf_geometry_indices;
+    SlimBVH bvh;
+} SlimSceneData;
+typedef struct {                                              /* core/base.h:1300-1311 */
+    uint32_t width_times_height;
+    float width_over_height, height_over_width, f_width, f_height, h_width, h_height;
+    uint16_t width, height, stride, _pad;
+} SlimDimensions;
+typedef struct { float r, g, b, opacity; } SlimPixel;          /* core/base.h:1081-1083 */
+typedef struct {                                              /* draw/canvas.h:11-17 */
+    SlimDimensions dimensions;
+    int32_t antialias;       /* SLIM_AA_* */
+    SlimPixel *pixels;
+    float *depths;
+} SlimCanvasData;
+typedef struct {                                              /* scene/camera.h:58-63 */
+    float inverted_camera_rotation[9];
+    SlimVec3 start, right, down, camera_position;
+    SlimVec2 C_start;
+    float squared_distance_to_projection_plane;
+    float sample_size;
+} SlimCameraRayProjection;
+typedef struct {                                              /* renderer/ray_tracer.h:10-17 */
+    uint8_t max_depth;
+    int8_t skybox_color_texture_id, skybox_radiance_texture_id, skybox_irradiance_texture_id;
+    int32_t render_mode;     /* SLIM_RENDER_* */
+    int32_t mip_level_colors[9];
+} SlimRayTracerSettings;
+
+/* Options with no reference counterpart (B200 execution choices). */
+enum { SLIM_ENGINE_WAVEFRONT = 0, SLIM_ENGINE_MEGAKERNEL = 1 };
+enum { SLIM_CONES_REFERENCE = 0, SLIM_CONES_PER_PIXEL = 1 };
+enum { SLIM_SCENE_BVH_UPLOADED = 0, SLIM_SCENE_BVH_REFIT = 1 };
+typedef struct {
+    int32_t engine;          /* SLIM_ENGINE_*: wavefront queues (default) or one fused kernel */
+    int32_t ray_cones;       /* SLIM_CONES_REFERENCE (default): the reference's effective ray
+                                cone (mip 0, see DESIGN); SLIM_CONES_PER_PIXEL: per-pixel spread */
+    int32_t scene_bvh;       /* SLIM_SCENE_BVH_UPLOADED (default) or GPU refit of its topology */
+    int32_t block_size;      /* threads per block, 0 = tuned default */
+    int32_t count_work;      /* non-zero: accumulate per-frame work counters (slower) */
+    int32_t _reserved[3];
+} SlimRenderOptions;
+
+/* Work counters of the last frame (rays traced and memory records touched). */
+typedef struct {
+    uint64_t primary_rays, shadow_rays, bounce_rays;
+    uint64_t scene_node_tests, mesh_node_tests, triangle_tests;
+    uint64_t geometry_tests, mesh_hit_fetches, texel_taps;
+    uint64_t pixels;
+} SlimWorkCounters;
+
+#ifdef __cplusplus
+#define SLIM_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define SLIM_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+SLIM_STATIC_ASSERT(sizeof(SlimGeometry) == 72, "Geometry is 72 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimMaterial) == 68, "Material is 68 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimLight) == 32, "Light is 32 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimBVHNode) == 32, "BVHNode is 32 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimTriangle) == 128, "Triangle is 128 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimTexelQuad) == 12, "TexelQuad is 12 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimTextureMip) == 16, "TextureMip is 16 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimTexture) == 40, "Texture is 40 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimMesh) == 128, "Mesh is 128 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimSceneData) == 184, "SceneData is 184 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimCanvasData) == 56, "CanvasData is 56 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimCameraRayProjection) == 100, "CameraRayProjection is 100 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimRayTracerSettings) == 44, "RayTracerSettings is 44 bytes");
+
+/* ======================================================================== *
+ * Drop-in hooks (renderer/renderer_GPU.h)                                   *
+ * ======================================================================== */
+
+/* Replaces initDataOnGPU(const Scene&) (renderer/renderer_GPU.h:180-281):
+ * one-time deep copy of the scene -- geometries, materials, lights, scene
+ * BVH, meshes (triangles + BVH nodes) and textures (mips + texel quads) --
+ * into the device layout.  Mesh and texture topology is frozen afterwards,
+ * as in the reference.  May be called again to replace the scene. */
+int slimInitDataOnGPU(const SlimSceneData *scene);
+
+/* Replace uploadLights/uploadCameras/uploadGeometries/uploadMaterials/
+ * uploadSceneBVH(const Scene&) (renderer/renderer_GPU.h:170-178): re-upload
+ * the per-frame mutable parts.  Counts must equal those given to
+ * slimInitDataOnGPU (SLIM_ERR_STATE otherwise). */
+int slimUploadLights(const SlimSceneData *scene);
+int slimUploadCameras(const SlimSceneData *scene);
+int slimUploadGeometries(const SlimSceneData *scene);
+int slimUploadMaterials(const SlimSceneData *scene);
+int slimUploadSceneBVH(const SlimSceneData *scene);
+
+/* Replaces renderOnGPU(const Canvas&, const CameraRayProjection&,
+ * const RayTracerSettings&) (renderer/renderer_GPU.h:148-168): traces every
+ * pixel (every sub-sample under SSAA) and writes canvas->pixels (Pixel
+ * {clamp(c)^2, 1}) and canvas->depths synchronously, like the reference. */
+int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                    const SlimRayTracerSettings *settings);
+
+/* ======================================================================== *
+ * Extensions (no reference counterpart unless cited)                        *
+ * ======================================================================== */
+
+const char *slimGetLastError(void);
+int slimGetVersion(void);
+
+int slimSetRenderOptions(const SlimRenderOptions *options);
+int slimGetRenderOptions(SlimRenderOptions *options);
+
+/* Device-resident render: same work as slimRenderOnGPU, but the frame stays
+ * in device memory (d_pixels: float4 per sample, d_depths: float per
+ * sample, both allocated by the caller with room for every sample) and the
+ * call is asynchronous on `stream` (a cudaStream_t, 0 = legacy default). */
+int slimRenderToDevice(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                       const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths,
+                       void *stream);
+
+/* Closest hit of every primary ray (renderer/ray_tracer.h:36-45 ->
+ * scene/scene_tracer.h:26-98) into device buffers of width*height entries:
+ * geometry index (-1 = miss), mesh triangle id in leaf order (0 for
+ * implicit primitives), hit distance, hit-from-behind flag. */
+int slimTracePrimary(const SlimCameraRayProjection *projection, int width, int height,
+                     void *d_geometry_ids, void *d_primitive_ids, void *d_distances,
+                     void *d_from_behind, void *stream);
+
+/* Work counters of the last frame rendered with options.count_work set. */
+int slimGetWorkCounters(SlimWorkCounters *counters);
+
+/* Re-fits the device copy of the scene BVH to the current geometries
+ * (GPU), keeping the topology last uploaded: scene/scene.h:165-191 rebuilds
+ * it from scratch on the host every frame instead. */
+int slimRefitSceneBVH(void *stream);
+
+/* Host-side helpers: the reference's own host algorithms, restated. */
+
+/* CameraRayProjection::reset (scene/camera.h:69-83); orientation given as
+ * the camera matrix columns X (right), Y (up), Z (forward). */
+int slimProjectionReset(const float orientation9[9], const float position3[3], float focal_length,
+                        int width, int height, int antialias_ssaa, SlimCameraRayProjection *out);
+
+/* Scene::updateAABBs + updateBVH (scene/scene.h:165-191, full SAH build with
+ * one geometry per leaf, scene/bvh_builder.h:10-263) into scene->bvh.nodes
+ * (capacity 2*geometries), scene->bvh_leaf_geometry_indices and
+ * scene->flags (SLIM_SCENE_HAD_EMISSIVE_QUADS, scene/scene.h:156-159). */
+int slimBuildSceneBVH(SlimSceneData *scene);
+
+/* obj2mesh after parsing (obj2mesh.cpp:201-231 with scale 1, no rotation)
+ * and BVHBuilder::buildMesh (scene/bvh_builder.h:265-341): recentres the
+ * positions (in place) on the AABB centre, builds the SAH BVH (at most 2
+ * triangles per leaf) and the leaf-ordered Triangle records.  Caller sizes
+ * out_triangles for triangle_count and out_nodes for 2*triangle_count. */
+int slimBuildMesh(float *positions, uint32_t vertex_count, const uint32_t *position_indices,
+                  uint32_t triangle_count, const float *normals, uint32_t normals_count,
+                  const uint32_t *normal_indices, const float *uvs, uint32_t uvs_count,
+                  const uint32_t *uv_indices, SlimTriangle *out_triangles, SlimBVHNode *out_nodes,
+                  uint32_t *out_node_count, uint32_t *out_height, float out_aabb6[6]);
+
+/* .mesh file I/O (serialization/mesh.h:56-163).  slimReadMeshHeader fills
+ * the counts; the caller then allocates the arrays it points the mesh at
+ * (triangles, positions, index arrays, edges, uvs, normals, bvh.nodes) and
+ * calls slimReadMesh.  Edge indices may be null on write (edge_count 0). */
+int slimReadMeshHeader(const char *path, SlimMesh *mesh);
+int slimReadMesh(const char *path, SlimMesh *mesh);
+int slimWriteMesh(const char *path, const SlimMesh *mesh);
+
+/* .texture file I/O (core/base.h:1544-1609, serialization/texture.h:7-62). */
+int slimReadTextureHeader(const char *path, SlimTexture *texture, uint32_t *total_texel_quads);
+int slimReadTexture(const char *path, SlimTexture *texture, SlimTextureMip *mips,
+                    SlimTexelQuad *texel_quads);
+int slimWriteTexture(const char *path, const SlimTexture *texture);
+
+/* bmp2texture's texel-quad baker (bmp2texture.cpp:24-237,255-335) from
+ * 8-bit BGR(A) rows as a BMP stores them after its own flip handling.
+ * flags: SLIM_IMAGE_* (LINEAR, MIPMAP, WRAP, NORMAL, CUBEMAP as the
+ * -l -m -w -n -c switches).  First call with texel_quads == NULL to get
+ * mip_count and the texel-quad count, then again with buffers. */
+int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels,
+                    uint32_t flags, SlimTexture *texture, SlimTextureMip *mips,
+                    SlimTexelQuad *texel_quads, uint32_t *mip_count, uint32_t *texel_quad_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLIMTRACER_B200_H */

@@ -1,0 +1,183 @@
+"""ctypes access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+  liboracle.so        plain-C restatement of the reference's trace path
+                      (oracle/slim_oracle.c), built by oracle/Makefile.
+  _ref/libslimref.so  the reference's own CPU code, compiled from its
+                      sources by oracle/build_ref.sh (present when it was
+                      built on a machine holding the reference sources).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
+reference legs use this module, as the checker and the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libslimref.so"
+
+P = C.c_void_p
+WORK_FIELDS = ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests",
+               "triangle_tests", "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels"]
+
+_oracle = None
+_ref = None
+
+
+def _ptr(a):
+    return 0 if a is None else (a.ctypes.data if isinstance(a, np.ndarray) else int(a))
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_LIB.exists():
+            import subprocess
+            subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+        h = C.CDLL(str(ORACLE_LIB))
+        h.oracle_render.argtypes = [P, P, P, P, C.c_int, C.c_int, C.c_int, P]
+        h.oracle_render.restype = C.c_int
+        h.oracle_trace_primary.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P]
+        h.oracle_trace_primary.restype = C.c_int
+        _oracle = h
+    return _oracle
+
+
+def reference_available():
+    return REF_LIB.exists()
+
+
+def reference():
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} not built (oracle/build_ref.sh needs the reference sources)")
+        h = C.CDLL(str(REF_LIB))
+        h.ref_projection_reset.argtypes = [P, P, C.c_float, C.c_int, C.c_int, C.c_int, P]
+        h.ref_build_scene_bvh.argtypes = [P]
+        h.ref_build_mesh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, P, P, P, P]
+        h.ref_render.argtypes = [P, P, P, P, C.c_int, C.c_int, C.c_int]
+        h.ref_render_cpu.argtypes = [P, P, P, P]
+        h.ref_trace_primary.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P, C.c_int]
+        for n in ["ref_projection_reset", "ref_build_scene_bvh", "ref_build_mesh", "ref_render", "ref_render_cpu",
+                  "ref_trace_primary"]:
+            getattr(h, n).restype = C.c_int
+        _ref = h
+    return _ref
+
+
+def make_canvas(width, height, antialias, layout):
+    """Host framebuffer + CanvasData record (draw/canvas.h:11-17)."""
+    s = 2 if antialias == 2 else 1
+    pixels = np.zeros((height * s * width * s, 4), np.float32)
+    depths = np.full(height * width * (1 if antialias == 0 else 4), np.inf, np.float32)
+    cv = np.zeros((), layout.CANVAS_DATA)
+    cv["width_times_height"] = width * height
+    cv["f_width"], cv["f_height"] = width, height
+    cv["h_width"], cv["h_height"] = width * 0.5, height * 0.5
+    cv["width_over_height"], cv["height_over_width"] = width / height, height / width
+    cv["width"], cv["height"], cv["stride"] = width, height, width
+    cv["antialias"] = antialias
+    cv["pixels"], cv["depths"] = pixels.ctypes.data, depths.ctypes.data
+    return cv, pixels, depths
+
+
+def oracle_render(scene, projection, settings, width, height, antialias=0, rows=None, cones_per_pixel=False,
+                  count=False, layout=None):
+    """Renders with the C restatement; returns (pixels, depths, counters)."""
+    cv, pixels, depths = make_canvas(width, height, antialias, layout)
+    s = 2 if antialias == 2 else 1
+    r0, r1 = (0, height * s) if rows is None else rows
+    counters = np.zeros(10, np.uint64) if count else None
+    rc = oracle().oracle_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, int(cones_per_pixel),
+                                _ptr(counters))
+    assert rc == 0, rc
+    work = None if counters is None else dict(zip(WORK_FIELDS, (int(c) for c in counters)))
+    return pixels, depths, work
+
+
+def reference_render(scene, projection, settings, width, height, antialias=0, rows=None, threads=None, layout=None):
+    cv, pixels, depths = make_canvas(width, height, antialias, layout)
+    s = 2 if antialias == 2 else 1
+    r0, r1 = (0, height * s) if rows is None else rows
+    threads = threads or os.cpu_count() or 1
+    rc = reference().ref_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, threads)
+    assert rc == 0, rc
+    return pixels, depths
+
+
+def reference_render_cpu(scene, projection, settings, width, height, layout=None):
+    """The reference's unmodified single-threaded renderOnCPU."""
+    cv, pixels, depths = make_canvas(width, height, 0, layout)
+    rc = reference().ref_render_cpu(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings))
+    assert rc == 0, rc
+    return pixels, depths
+
+
+def _primary(fn, scene, projection, width, height, *extra):
+    n = width * height
+    g = np.zeros(n, np.int32)
+    p = np.zeros(n, np.uint32)
+    d = np.zeros(n, np.float32)
+    b = np.zeros(n, np.uint8)
+    rc = fn(scene.ptr, _ptr(projection), width, height, _ptr(g), _ptr(p), _ptr(d), _ptr(b), *extra)
+    assert rc == 0, rc
+    return g, p, d, b
+
+
+def oracle_trace_primary(scene, projection, width, height):
+    return _primary(oracle().oracle_trace_primary, scene, projection, width, height)
+
+
+def reference_trace_primary(scene, projection, width, height, threads=None):
+    return _primary(reference().ref_trace_primary, scene, projection, width, height, threads or os.cpu_count() or 1)
+
+
+def reference_projection(camera, width, height, ssaa, layout):
+    out = np.zeros((), layout.PROJECTION)
+    o = np.ascontiguousarray(camera.orientation, np.float32)
+    p = np.ascontiguousarray(camera.position, np.float32)
+    rc = reference().ref_projection_reset(_ptr(o), _ptr(p), C.c_float(camera.focal_length), width, height, int(ssaa),
+                                          _ptr(out))
+    assert rc == 0
+    return out
+
+
+def reference_scene_bvh(scene, layout):
+    """Runs the reference's Scene BVH build on a copy of the scene data;
+    returns (nodes, leaf_ids, flags, height)."""
+    g = int(scene.data["counts"][0])
+    nodes = np.zeros(2 * g, layout.BVH_NODE)
+    leaf = np.zeros(g, np.uint32)
+    sd = scene.data.copy()
+    sd["bvh_nodes"], sd["bvh_leaf_geometry_indices"] = nodes.ctypes.data, leaf.ctypes.data
+    rc = reference().ref_build_scene_bvh(_ptr(sd))
+    assert rc == 0
+    return nodes[:int(sd["bvh_node_count"])], leaf, int(sd["flags"]), int(sd["bvh_height"])
+
+
+def reference_build_mesh(positions, indices, normals=None, normal_indices=None, uvs=None, uv_indices=None,
+                         layout=None):
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    t = len(idx)
+    nrm = None if normals is None else np.ascontiguousarray(normals, np.float32)
+    nidx = None if normal_indices is None else np.ascontiguousarray(normal_indices, np.uint32)
+    uv = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
+    uidx = None if uv_indices is None else np.ascontiguousarray(uv_indices, np.uint32)
+    tris = np.zeros(t, layout.TRIANGLE)
+    nodes = np.zeros(2 * t + 2, layout.BVH_NODE)
+    nc = np.zeros(1, np.uint32)
+    ht = np.zeros(1, np.uint32)
+    aabb = np.zeros(6, np.float32)
+    out_pos = np.zeros_like(pos)
+    rc = reference().ref_build_mesh(_ptr(pos), len(pos), _ptr(idx), t, _ptr(nrm), 0 if nrm is None else len(nrm),
+                                    _ptr(nidx), _ptr(uv), 0 if uv is None else len(uv), _ptr(uidx), _ptr(tris),
+                                    _ptr(nodes), _ptr(nc), _ptr(ht), _ptr(aabb), _ptr(out_pos))
+    assert rc == 0
+    return tris, nodes[:int(nc[0])], int(ht[0]), aabb, out_pos

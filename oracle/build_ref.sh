@@ -1,0 +1,56 @@
+#!/usr/bin/env bash
+# Builds the reference renderer's CPU path into oracle/_ref/ (TEST
+# INFRASTRUCTURE: the checker and the timed CPU baseline, never the product).
+#
+# The reference (HardCoreCodin/SlimTracinCpp) is MSVC/Win32-only as shipped.
+# Its sources are read where they lie, copied to a temporary directory and
+# given three portability patches there; nothing of them enters this
+# repository and the temporary copy is deleted after the build:
+#   1. core/base.h: `u32`/`i32` are `unsigned/signed long int`, 8 bytes on
+#      LP64, which breaks every binary layout -> `unsigned/signed int`.
+#   2. math/mat3.h: GCC rejects vec3 members in mat3's anonymous union of
+#      {X,Y,Z} and {right,up,forward} -> plain `vec3 X, Y, Z;`, and the
+#      only users of the aliases (scene/camera.h) renamed to X/Y/Z.
+#   3. unqualified abs/sqrt/pow on floats: force-included ref/ref_shim.h
+#      (no source edit).
+# Flags: -mfma so the reference's fast_mul_add is fmaf (FP_FAST_FMAF), and
+# -ffp-contract=off so nothing else is fused -- the floating-point policy the
+# CUDA kernels follow (-fmad=false with explicit fmaf at the same sites).
+# -ftrivial-auto-var-init=zero makes the reference's reads of never-written
+# locals deterministic (hitsDefaultTetrahedron copies a local RayHit whose
+# scaling_factor/id it never sets, core/ray.h:223,304-306): they read 0, the
+# value every other never-written tracer member has in the reference app.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF_SRC="${SLIM_REFERENCE_SRC:-/root/reference/src}"
+OUT="$HERE/_ref"
+if [ ! -d "$REF_SRC/slim" ]; then
+    echo "build_ref.sh: reference sources not found at $REF_SRC" >&2
+    exit 2
+fi
+mkdir -p "$OUT"
+TMP="$(mktemp -d)"
+trap 'rm -rf "$TMP"' EXIT
+cp -r "$REF_SRC/slim" "$TMP/slim"
+sed -i -e 's/typedef unsigned long int  u32;/typedef unsigned int u32;/' \
+       -e 's/typedef signed   long int  i32;/typedef signed int i32;/' "$TMP/slim/core/base.h"
+grep -q 'typedef unsigned int u32;' "$TMP/slim/core/base.h"
+grep -q 'typedef signed int i32;' "$TMP/slim/core/base.h"
+python3 - "$TMP/slim/math/mat3.h" <<'EOF'
+import sys, re
+p = sys.argv[1]
+s = open(p).read()
+pat = re.compile(r"union\s*\{\s*struct\s*\{\s*vec3 X, Y, Z;\s*\};\s*struct\s*\{\s*vec3 right, up, forward;\s*\};\s*\};")
+s2, n = pat.subn("vec3 X, Y, Z;", s)
+assert n == 1, "mat3 union not found"
+open(p, "w").write(s2)
+EOF
+sed -i -e 's/orientation\.right/orientation.X/g' -e 's/orientation\.up/orientation.Y/g' \
+       -e 's/orientation\.forward/orientation.Z/g' "$TMP/slim/scene/camera.h"
+
+CXXFLAGS=(-std=c++17 -O3 -march=x86-64-v3 -mfma -ffp-contract=off -fno-fast-math -DNDEBUG
+          -ftrivial-auto-var-init=zero
+          -fPIC -pthread -w -include "$HERE/ref/ref_shim.h" -I "$TMP")
+g++ "${CXXFLAGS[@]}" -shared -o "$OUT/libslimref.so.tmp" "$HERE/ref/ref_driver.cpp"
+mv "$OUT/libslimref.so.tmp" "$OUT/libslimref.so"
+echo "built $OUT/libslimref.so"

@@ -1,0 +1,717 @@
+// C ABI of libslimtracer_b200: the drop-in hooks of renderer/renderer_GPU.h
+// plus the device-resident extensions.  One process-wide render context,
+// like the reference's module-global GPU mirror (renderer/renderer_GPU.h:
+// 12-20); calls are serialised by a mutex.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "slimtracer_b200.h"
+#include "device_scene.h"
+#include "host_common.h"
+#include "kernels.h"
+
+namespace slim {
+
+namespace {
+thread_local std::string g_error;
+}
+int set_error(int code, const char *message) {
+    g_error = message ? message : "";
+    return code;
+}
+const char *last_error() { return g_error.c_str(); }
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return set_error(SLIM_ERR_CUDA, m.c_str());
+}
+#define SLIM_CUDA(call, what) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return cuda_fail(e_, what); } while (0)
+
+template <typename T>
+struct DevArray {
+    T *ptr = nullptr;
+    size_t count = 0;
+    int reserve(size_t n, const char *what) {
+        if (n <= count && ptr) return SLIM_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+        if (!n) return SLIM_OK;
+        SLIM_CUDA(cudaMalloc(&ptr, n * sizeof(T)), what);
+        count = n;
+        return SLIM_OK;
+    }
+    void release() { if (ptr) cudaFree(ptr); ptr = nullptr; count = 0; }
+};
+
+struct Context {
+    bool initialized = false;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    SlimSceneCounts counts{};
+    std::vector<SlimGeometry> geometries;
+    std::vector<SlimMaterial> materials;
+    uint32_t max_mesh_height = 0;
+
+    DevArray<float4> d_geometries, d_scene_nodes, d_mesh_nodes, d_tri_hot, d_tri_cold;
+    DevArray<SlimMaterial> d_materials;
+    DevArray<SlimLight> d_lights;
+    DevArray<uint32_t> d_leaf_geometry, d_emissive_quads, d_refit_order;
+    DevArray<DevMesh> d_meshes;
+    DevArray<DevTexture> d_textures;
+    DevArray<DevMip> d_mips;
+    DevArray<uint4> d_quads;
+    DevArray<float4> d_pixels;
+    DevArray<float> d_depths;
+    DevArray<uint32_t> d_error;
+    DevArray<unsigned long long> d_counters;
+    std::vector<uint32_t> refit_order;
+    uint32_t scene_node_count = 0;
+
+    DevScene scene{};
+    SlimRenderOptions options{};
+    SlimWorkCounters last_counters{};
+    WavefrontBuffers wavefront{};
+    DevArray<float4> w_color, w_through, w_next, w_rays0, w_rays1, w_hits, w_shadow_rays;
+    DevArray<uint32_t> w_counts, w_shadow_meta, w_shadow_mask;
+};
+
+Context g_ctx;
+std::mutex g_mutex;
+
+int ensure_device(Context &c) {
+    if (c.device >= 0) return SLIM_OK;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return set_error(SLIM_ERR_CUDA, "no CUDA device: libslimtracer_b200 has no CPU path");
+    SLIM_CUDA(cudaGetDevice(&c.device), "cudaGetDevice");
+    SLIM_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    int rc = c.d_error.reserve(1, "alloc error flags");
+    if (rc) return rc;
+    rc = c.d_counters.reserve(16, "alloc counters");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemset(c.d_error.ptr, 0, sizeof(uint32_t)), "clear error flags");
+    return SLIM_OK;
+}
+
+// Geometry record: rotation | position,type | scale,material | 1/scale,flags+mesh<<8.
+// 1/scale is the IEEE quotient Ray::localize computes (core/ray.h:30).
+void pack_geometry(const SlimGeometry &g, float4 out[4]) {
+    const SlimTransform &t = g.transform;
+    uint32_t type = (uint32_t)g.type, bits = (uint32_t)g.flags | ((g.type == SLIM_GEOMETRY_MESH ? g.id : 0u) << 8);
+    float ft, fm, fb;
+    memcpy(&ft, &type, 4);
+    memcpy(&fm, &g.material_id, 4);
+    memcpy(&fb, &bits, 4);
+    out[0] = make_float4(t.orientation.axis.x, t.orientation.axis.y, t.orientation.axis.z, t.orientation.amount);
+    out[1] = make_float4(t.position.x, t.position.y, t.position.z, ft);
+    out[2] = make_float4(t.scale.x, t.scale.y, t.scale.z, fm);
+    out[3] = make_float4(1.0f / t.scale.x, 1.0f / t.scale.y, 1.0f / t.scale.z, fb);
+}
+
+int check_scene_arrays(const SlimSceneData *s) {
+    if (!s) return set_error(SLIM_ERR_ARGUMENT, "scene is null");
+    const SlimSceneCounts &n = s->counts;
+    if (!n.geometries || !s->geometries) return set_error(SLIM_ERR_ARGUMENT, "scene has no geometries");
+    if (!n.materials || !s->materials) return set_error(SLIM_ERR_ARGUMENT, "scene has no materials");
+    if (n.lights && !s->lights) return set_error(SLIM_ERR_ARGUMENT, "scene lights array missing");
+    if (n.lights > (uint32_t)kMaxLights) return set_error(SLIM_ERR_LIMIT, "more lights than supported (64)");
+    if (n.meshes && !s->meshes) return set_error(SLIM_ERR_ARGUMENT, "scene meshes array missing");
+    if (n.textures && !s->textures) return set_error(SLIM_ERR_ARGUMENT, "scene textures array missing");
+    if (n.geometries > (1u << 24)) return set_error(SLIM_ERR_LIMIT, "too many geometries");
+    for (uint32_t g = 0; g < n.geometries; g++) {
+        const SlimGeometry &geo = s->geometries[g];
+        if (geo.material_id >= n.materials) return set_error(SLIM_ERR_ARGUMENT, "geometry material_id out of range");
+        if (geo.type == SLIM_GEOMETRY_MESH && geo.id >= n.meshes) return set_error(SLIM_ERR_ARGUMENT, "geometry mesh id out of range");
+    }
+    for (uint32_t m = 0; m < n.materials; m++) {
+        const SlimMaterial &mat = s->materials[m];
+        for (uint32_t k = 0; k < mat.texture_count && k < 2; k++)
+            if (mat.texture_ids[k] >= n.textures && (mat.flags & (SLIM_MATERIAL_HAS_ALBEDO_MAP | SLIM_MATERIAL_HAS_NORMAL_MAP)))
+                return set_error(SLIM_ERR_ARGUMENT, "material texture id out of range");
+    }
+    return SLIM_OK;
+}
+
+// BVH topology checks that make every device traversal terminate and stay
+// in bounds: inner nodes point strictly forward to an adjacent child pair,
+// leaves point inside the primitive array, and the height fits the stack.
+int check_bvh(const SlimBVHNode *nodes, uint32_t node_count, uint32_t primitive_count, uint32_t height, const char *what) {
+    if (!nodes || !node_count) return set_error(SLIM_ERR_ARGUMENT, what);
+    if (height + 2 > (uint32_t)kStackCapacity) return set_error(SLIM_ERR_LIMIT, "BVH deeper than the traversal stack (62 levels)");
+    for (uint32_t i = 0; i < node_count; i++) {
+        const SlimBVHNode &n = nodes[i];
+        if (n.leaf_count) {
+            if ((uint64_t)n.first_index + n.leaf_count > primitive_count) return set_error(SLIM_ERR_ARGUMENT, what);
+        } else if (n.first_index <= i || (uint64_t)n.first_index + 1 >= node_count) {
+            return set_error(SLIM_ERR_ARGUMENT, what);
+        }
+    }
+    return SLIM_OK;
+}
+
+// Depth of the deepest node reachable from the root (the traversal stack
+// bound) -- the stored height byte is not trusted.
+uint32_t bvh_depth(const SlimBVHNode *nodes, uint32_t node_count) {
+    std::vector<uint32_t> depth(node_count, 0);
+    uint32_t deepest = 1;
+    depth[0] = 1;
+    for (uint32_t i = 0; i < node_count; i++) {
+        if (!depth[i] || nodes[i].leaf_count) continue;
+        uint32_t c = nodes[i].first_index;
+        depth[c] = depth[c + 1] = depth[i] + 1;
+        if (depth[i] + 1 > deepest) deepest = depth[i] + 1;
+    }
+    return deepest;
+}
+
+int upload_emissive(Context &c) {
+    std::vector<uint32_t> list;
+    for (uint32_t g = 0; g < c.counts.geometries; g++) {
+        const SlimGeometry &geo = c.geometries[g];
+        if (geo.type == SLIM_GEOMETRY_QUAD && (c.materials[geo.material_id].flags & SLIM_MATERIAL_IS_EMISSIVE))
+            list.push_back(g);
+    }
+    c.scene.emissive_quad_count = (uint32_t)list.size();
+    int rc = c.d_emissive_quads.reserve(list.size() ? list.size() : 1, "alloc emissive list");
+    if (rc) return rc;
+    if (!list.empty())
+        SLIM_CUDA(cudaMemcpy(c.d_emissive_quads.ptr, list.data(), list.size() * 4, cudaMemcpyHostToDevice), "upload emissive list");
+    c.scene.emissive_quads = c.d_emissive_quads.ptr;
+    return SLIM_OK;
+}
+
+int upload_geometries(Context &c, const SlimSceneData *s) {
+    uint32_t n = c.counts.geometries;
+    for (uint32_t g = 0; g < n; g++) {
+        const SlimGeometry &geo = s->geometries[g];
+        if (geo.material_id >= c.counts.materials) return set_error(SLIM_ERR_ARGUMENT, "geometry material_id out of range");
+        if (geo.type == SLIM_GEOMETRY_MESH && geo.id >= c.counts.meshes) return set_error(SLIM_ERR_ARGUMENT, "geometry mesh id out of range");
+    }
+    c.geometries.assign(s->geometries, s->geometries + n);
+    std::vector<float4> packed(4 * (size_t)n);
+    for (uint32_t g = 0; g < n; g++) pack_geometry(c.geometries[g], &packed[4 * (size_t)g]);
+    int rc = c.d_geometries.reserve(packed.size(), "alloc geometries");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(c.d_geometries.ptr, packed.data(), packed.size() * sizeof(float4), cudaMemcpyHostToDevice),
+              "upload geometries");
+    c.scene.geometries = c.d_geometries.ptr;
+    return upload_emissive(c);
+}
+
+int upload_materials(Context &c, const SlimSceneData *s) {
+    uint32_t n = c.counts.materials;
+    for (uint32_t m = 0; m < n; m++) {
+        const SlimMaterial &mat = s->materials[m];
+        for (uint32_t k = 0; k < mat.texture_count && k < 2; k++)
+            if (mat.texture_ids[k] >= c.counts.textures && (mat.flags & (SLIM_MATERIAL_HAS_ALBEDO_MAP | SLIM_MATERIAL_HAS_NORMAL_MAP)))
+                return set_error(SLIM_ERR_ARGUMENT, "material texture id out of range");
+    }
+    c.materials.assign(s->materials, s->materials + n);
+    int rc = c.d_materials.reserve(n, "alloc materials");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(c.d_materials.ptr, s->materials, n * sizeof(SlimMaterial), cudaMemcpyHostToDevice), "upload materials");
+    c.scene.materials = c.d_materials.ptr;
+    return c.geometries.empty() ? SLIM_OK : upload_emissive(c);
+}
+
+int upload_lights(Context &c, const SlimSceneData *s) {
+    uint32_t n = c.counts.lights;
+    int rc = c.d_lights.reserve(n ? n : 1, "alloc lights");
+    if (rc) return rc;
+    if (n) SLIM_CUDA(cudaMemcpy(c.d_lights.ptr, s->lights, n * sizeof(SlimLight), cudaMemcpyHostToDevice), "upload lights");
+    c.scene.lights = c.d_lights.ptr;
+    c.scene.light_count = n;
+    return SLIM_OK;
+}
+
+// Parent-before-child order of the scene BVH's inner nodes, reversed, so the
+// refit kernel can process it level by level bottom-up in one launch.
+void build_refit_order(Context &c, const SlimBVHNode *nodes, uint32_t node_count) {
+    c.refit_order.clear();
+    for (uint32_t i = 0; i < node_count; i++)
+        if (!nodes[i].leaf_count) c.refit_order.push_back(i);
+}
+
+int upload_scene_bvh(Context &c, const SlimSceneData *s) {
+    uint32_t n = s->bvh.node_count;
+    int rc = check_bvh(s->bvh.nodes, n, c.counts.geometries, 0, "scene BVH malformed");
+    if (rc) return rc;
+    if (!s->bvh_leaf_geometry_indices) return set_error(SLIM_ERR_ARGUMENT, "scene BVH leaf indices missing");
+    if (bvh_depth(s->bvh.nodes, n) + 2 > (uint32_t)kStackCapacity) return set_error(SLIM_ERR_LIMIT, "scene BVH deeper than the traversal stack");
+    for (uint32_t g = 0; g < c.counts.geometries; g++)
+        if (s->bvh_leaf_geometry_indices[g] >= c.counts.geometries) return set_error(SLIM_ERR_ARGUMENT, "scene BVH leaf index out of range");
+    rc = c.d_scene_nodes.reserve(2 * (size_t)n, "alloc scene BVH");
+    if (rc) return rc;
+    rc = c.d_leaf_geometry.reserve(c.counts.geometries, "alloc leaf indices");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(c.d_scene_nodes.ptr, s->bvh.nodes, n * sizeof(SlimBVHNode), cudaMemcpyHostToDevice), "upload scene BVH");
+    SLIM_CUDA(cudaMemcpy(c.d_leaf_geometry.ptr, s->bvh_leaf_geometry_indices, c.counts.geometries * 4, cudaMemcpyHostToDevice),
+              "upload leaf indices");
+    build_refit_order(c, s->bvh.nodes, n);
+    rc = c.d_refit_order.reserve(c.refit_order.size() ? c.refit_order.size() : 1, "alloc refit order");
+    if (rc) return rc;
+    if (!c.refit_order.empty())
+        SLIM_CUDA(cudaMemcpy(c.d_refit_order.ptr, c.refit_order.data(), c.refit_order.size() * 4, cudaMemcpyHostToDevice),
+                  "upload refit order");
+    c.scene_node_count = n;
+    c.scene.scene_nodes = c.d_scene_nodes.ptr;
+    c.scene.leaf_geometry = c.d_leaf_geometry.ptr;
+    c.scene.scene_node_count = n;
+    c.scene.flags = s->flags;
+    return SLIM_OK;
+}
+
+int upload_meshes(Context &c, const SlimSceneData *s) {
+    uint32_t n = c.counts.meshes;
+    std::vector<DevMesh> metas(n ? n : 1);
+    size_t total_nodes = 0, total_tris = 0;
+    c.max_mesh_height = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const SlimMesh &m = s->meshes[i];
+        if (!m.triangles || !m.triangle_count) return set_error(SLIM_ERR_ARGUMENT, "mesh has no triangles");
+        int rc = check_bvh(m.bvh.nodes, m.bvh.node_count, m.triangle_count, 0, "mesh BVH malformed");
+        if (rc) return rc;
+        uint32_t d = bvh_depth(m.bvh.nodes, m.bvh.node_count);
+        if (d + 2 > (uint32_t)kStackCapacity) return set_error(SLIM_ERR_LIMIT, "mesh BVH deeper than the traversal stack (62 levels)");
+        if (d > c.max_mesh_height) c.max_mesh_height = d;
+        DevMesh &dm = metas[i];
+        memset(&dm, 0, sizeof(dm));
+        dm.aabb_min[0] = m.aabb.min.x; dm.aabb_min[1] = m.aabb.min.y; dm.aabb_min[2] = m.aabb.min.z;
+        dm.aabb_max[0] = m.aabb.max.x; dm.aabb_max[1] = m.aabb.max.y; dm.aabb_max[2] = m.aabb.max.z;
+        dm.node_offset = (uint32_t)total_nodes;
+        dm.tri_offset = (uint32_t)total_tris;
+        dm.tri_count = m.triangle_count;
+        dm.node_count = m.bvh.node_count;
+        dm.has_normals = m.normals_count != 0;
+        dm.has_uvs = m.uvs_count != 0;
+        total_nodes += m.bvh.node_count;
+        total_tris += m.triangle_count;
+        if (total_nodes > 0xFFFFFFFFull / 2 || total_tris > 0xFFFFFFFFull / 4) return set_error(SLIM_ERR_LIMIT, "meshes too large");
+    }
+    int rc = c.d_meshes.reserve(metas.size(), "alloc meshes");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(c.d_meshes.ptr, metas.data(), metas.size() * sizeof(DevMesh), cudaMemcpyHostToDevice), "upload meshes");
+    c.scene.meshes = c.d_meshes.ptr;
+    c.scene.mesh_count = n;
+    if (!n) {
+        c.scene.mesh_nodes = nullptr;
+        c.scene.tri_hot = c.scene.tri_cold = nullptr;
+        return SLIM_OK;
+    }
+    rc = c.d_mesh_nodes.reserve(2 * total_nodes, "alloc mesh nodes");
+    if (rc) return rc;
+    rc = c.d_tri_hot.reserve(3 * total_tris, "alloc triangles");
+    if (rc) return rc;
+    rc = c.d_tri_cold.reserve(4 * total_tris, "alloc triangle attributes");
+    if (rc) return rc;
+    std::vector<float4> hot, cold;
+    for (uint32_t i = 0; i < n; i++) {
+        const SlimMesh &m = s->meshes[i];
+        const DevMesh &dm = metas[i];
+        SLIM_CUDA(cudaMemcpy(c.d_mesh_nodes.ptr + 2 * (size_t)dm.node_offset, m.bvh.nodes, m.bvh.node_count * sizeof(SlimBVHNode),
+                             cudaMemcpyHostToDevice), "upload mesh nodes");
+        hot.resize(3 * (size_t)m.triangle_count);
+        cold.resize(4 * (size_t)m.triangle_count);
+        for (uint32_t t = 0; t < m.triangle_count; t++) {
+            const SlimTriangle &tr = m.triangles[t];
+            const float *l = tr.local_to_tangent;
+            hot[3 * t + 0] = make_float4(tr.position.x, tr.position.y, tr.position.z, tr.normal.x);
+            hot[3 * t + 1] = make_float4(tr.normal.y, tr.normal.z, l[0], l[1]);
+            hot[3 * t + 2] = make_float4(l[3], l[4], l[6], l[7]);
+            cold[4 * t + 0] = make_float4(tr.n1.x, tr.n1.y, tr.n1.z, tr.n2.x);
+            cold[4 * t + 1] = make_float4(tr.n2.y, tr.n2.z, tr.n3.x, tr.n3.y);
+            cold[4 * t + 2] = make_float4(tr.n3.z, tr.uv1.x, tr.uv1.y, tr.uv2.x);
+            cold[4 * t + 3] = make_float4(tr.uv2.y, tr.uv3.x, tr.uv3.y, tr.uv_coverage);
+        }
+        SLIM_CUDA(cudaMemcpy(c.d_tri_hot.ptr + 3 * (size_t)dm.tri_offset, hot.data(), hot.size() * sizeof(float4),
+                             cudaMemcpyHostToDevice), "upload triangles");
+        SLIM_CUDA(cudaMemcpy(c.d_tri_cold.ptr + 4 * (size_t)dm.tri_offset, cold.data(), cold.size() * sizeof(float4),
+                             cudaMemcpyHostToDevice), "upload triangle attributes");
+    }
+    c.scene.mesh_nodes = c.d_mesh_nodes.ptr;
+    c.scene.tri_hot = c.d_tri_hot.ptr;
+    c.scene.tri_cold = c.d_tri_cold.ptr;
+    return SLIM_OK;
+}
+
+int upload_textures(Context &c, const SlimSceneData *s) {
+    uint32_t n = c.counts.textures;
+    c.scene.texture_count = n;
+    if (!n) {
+        c.scene.textures = nullptr;
+        c.scene.mips = nullptr;
+        c.scene.quads = nullptr;
+        return SLIM_OK;
+    }
+    std::vector<DevTexture> texs(n);
+    std::vector<DevMip> mips;
+    size_t total_quads = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const SlimTexture &t = s->textures[i];
+        bool cube = (t.flags & SLIM_IMAGE_CUBEMAP) != 0;
+        if (!t.mips || !t.mip_count || (cube && t.mip_count < 3)) return set_error(SLIM_ERR_ARGUMENT, "texture has no mips");
+        DevTexture &dt = texs[i];
+        memset(&dt, 0, sizeof(dt));
+        dt.width = t.width; dt.height = t.height; dt.mip_count = t.mip_count; dt.flags = t.flags;
+        dt.mip_base = (uint32_t)mips.size();
+        for (uint32_t m = 0; m < t.mip_count; m++) {
+            const SlimTextureMip &mip = t.mips[m];
+            if (!mip.texel_quads || !mip.width || !mip.height) return set_error(SLIM_ERR_ARGUMENT, "texture mip empty");
+            DevMip dm{mip.width, mip.height, (uint32_t)total_quads, 0};
+            mips.push_back(dm);
+            total_quads += (size_t)(mip.width + 1) * (mip.height + 1);
+            if (total_quads > 0xFFFFFFFFull) return set_error(SLIM_ERR_LIMIT, "textures too large");
+        }
+    }
+    int rc = c.d_textures.reserve(n, "alloc textures");
+    if (rc) return rc;
+    rc = c.d_mips.reserve(mips.size(), "alloc mips");
+    if (rc) return rc;
+    rc = c.d_quads.reserve(total_quads, "alloc texel quads");
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(c.d_textures.ptr, texs.data(), n * sizeof(DevTexture), cudaMemcpyHostToDevice), "upload textures");
+    SLIM_CUDA(cudaMemcpy(c.d_mips.ptr, mips.data(), mips.size() * sizeof(DevMip), cudaMemcpyHostToDevice), "upload mips");
+    std::vector<uint4> quads;
+    for (uint32_t i = 0; i < n; i++) {
+        const SlimTexture &t = s->textures[i];
+        for (uint32_t m = 0; m < t.mip_count; m++) {
+            const SlimTextureMip &mip = t.mips[m];
+            size_t q = (size_t)(mip.width + 1) * (mip.height + 1);
+            quads.resize(q);
+            for (size_t k = 0; k < q; k++) {
+                const SlimTexelQuad &src = mip.texel_quads[k];
+                uint4 v;
+                memcpy(&v.x, src.R, 4);
+                memcpy(&v.y, src.G, 4);
+                memcpy(&v.z, src.B, 4);
+                v.w = 0;
+                quads[k] = v;
+            }
+            SLIM_CUDA(cudaMemcpy(c.d_quads.ptr + mips[texs[i].mip_base + m].quad_offset, quads.data(), q * sizeof(uint4),
+                                 cudaMemcpyHostToDevice), "upload texel quads");
+        }
+    }
+    c.scene.textures = c.d_textures.ptr;
+    c.scene.mips = c.d_mips.ptr;
+    c.scene.quads = c.d_quads.ptr;
+    return SLIM_OK;
+}
+
+int require_init(Context &c, const SlimSceneData *s) {
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!s) return set_error(SLIM_ERR_ARGUMENT, "scene is null");
+    return SLIM_OK;
+}
+
+int check_settings(const Context &c, const SlimRayTracerSettings *st) {
+    int8_t ids[3] = {st->skybox_color_texture_id, st->skybox_radiance_texture_id, st->skybox_irradiance_texture_id};
+    for (int8_t id : ids) {
+        if (id < 0) continue;
+        if ((uint32_t)id >= c.counts.textures) return set_error(SLIM_ERR_ARGUMENT, "skybox texture id out of range");
+    }
+    if (st->render_mode == SLIM_RENDER_MIP_LEVEL)
+        for (int k = 0; k < 9; k++)
+            if (st->mip_level_colors[k] < 0 || st->mip_level_colors[k] > 35) return set_error(SLIM_ERR_ARGUMENT, "bad mip level color");
+    return SLIM_OK;
+}
+
+int ensure_wavefront(Context &c, uint32_t samples);
+
+int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+           const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream) {
+    const SlimDimensions &dim = canvas->dimensions;
+    if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
+    if (canvas->antialias < SLIM_AA_NONE || canvas->antialias > SLIM_AA_SSAA) return set_error(SLIM_ERR_ARGUMENT, "bad antialias mode");
+    int rc = check_settings(c, settings);
+    if (rc) return rc;
+    uint32_t s = canvas->antialias == SLIM_AA_SSAA ? 2 : 1;
+    DevFrame F;
+    memset(&F, 0, sizeof(F));
+    F.projection = *projection;
+    F.settings = *settings;
+    F.width = (uint32_t)dim.width * s;
+    F.height = (uint32_t)dim.height * s;
+    F.stride = dim.stride ? dim.stride : dim.width;
+    if (F.stride < dim.width) return set_error(SLIM_ERR_ARGUMENT, "canvas stride below width");
+    F.antialias = canvas->antialias;
+    F.cones_per_pixel = c.options.ray_cones == SLIM_CONES_PER_PIXEL;
+    F.pixels = d_pixels;
+    F.depths = d_depths;
+    F.error_flags = c.d_error.ptr;
+    F.counters = c.options.count_work ? c.d_counters.ptr : nullptr;
+    if (F.counters) SLIM_CUDA(cudaMemsetAsync(F.counters, 0, 16 * sizeof(unsigned long long), stream), "clear counters");
+    cudaError_t e;
+    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) {
+        e = launch_render_fused(c.scene, F, c.options.block_size, stream);
+    } else {
+        rc = ensure_wavefront(c, F.width * F.height);
+        if (rc) return rc;
+        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "render launch");
+    return SLIM_OK;
+}
+
+int ensure_wavefront(Context &c, uint32_t samples) {
+    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= samples) return SLIM_OK;
+    uint32_t n = samples;
+    int rc = 0;
+    if ((rc = c.w_color.reserve(n, "alloc path color"))) return rc;
+    if ((rc = c.w_through.reserve(n, "alloc path throughput"))) return rc;
+    if ((rc = c.w_next.reserve(n, "alloc path next throughput"))) return rc;
+    if ((rc = c.w_rays0.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
+    if ((rc = c.w_rays1.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
+    if ((rc = c.w_hits.reserve(4 * (size_t)n, "alloc hit records"))) return rc;
+    if ((rc = c.w_shadow_rays.reserve(2 * (size_t)n, "alloc shadow queue"))) return rc;
+    if ((rc = c.w_counts.reserve(8, "alloc queue counters"))) return rc;
+    if ((rc = c.w_shadow_meta.reserve(n, "alloc shadow queue"))) return rc;
+    if ((rc = c.w_shadow_mask.reserve(n, "alloc shadow masks"))) return rc;
+    WavefrontBuffers &B = c.wavefront;
+    B.path_color = c.w_color.ptr;
+    B.path_throughput = c.w_through.ptr;
+    B.path_next = c.w_next.ptr;
+    B.rays[0] = c.w_rays0.ptr;
+    B.rays[1] = c.w_rays1.ptr;
+    B.queue_count = c.w_counts.ptr;
+    B.hits = c.w_hits.ptr;
+    B.shadow_rays = c.w_shadow_rays.ptr;
+    B.shadow_meta = c.w_shadow_meta.ptr;
+    B.shadow_mask = c.w_shadow_mask.ptr;
+    B.capacity = n;
+    B.shadow_capacity = n;
+    return SLIM_OK;
+}
+
+int read_errors(Context &c, cudaStream_t stream) {
+    uint32_t flags = 0;
+    SLIM_CUDA(cudaMemcpyAsync(&flags, c.d_error.ptr, 4, cudaMemcpyDeviceToHost, stream), "read error flags");
+    SLIM_CUDA(cudaStreamSynchronize(stream), "render");
+    if (flags) {
+        SLIM_CUDA(cudaMemset(c.d_error.ptr, 0, 4), "clear error flags");
+        if (flags & kErrStack) return set_error(SLIM_ERR_STACK, "a traversal stack overflowed on the device");
+        return set_error(SLIM_ERR_STATE, "device reported an index error");
+    }
+    return SLIM_OK;
+}
+
+int read_counters(Context &c, cudaStream_t stream) {
+    if (!c.options.count_work) return SLIM_OK;
+    unsigned long long v[16];
+    SLIM_CUDA(cudaMemcpyAsync(v, c.d_counters.ptr, sizeof(v), cudaMemcpyDeviceToHost, stream), "read counters");
+    SLIM_CUDA(cudaStreamSynchronize(stream), "read counters");
+    SlimWorkCounters &w = c.last_counters;
+    w.primary_rays = v[0]; w.shadow_rays = v[1]; w.bounce_rays = v[2];
+    w.scene_node_tests = v[3]; w.mesh_node_tests = v[4]; w.triangle_tests = v[5];
+    w.geometry_tests = v[6]; w.mesh_hit_fetches = v[7]; w.texel_taps = v[8];
+    w.pixels = v[0];
+    return SLIM_OK;
+}
+
+}  // namespace
+}  // namespace slim
+
+using namespace slim;
+
+extern "C" {
+
+int slimGetVersion(void) { return 1; }
+const char *slimGetLastError(void) { return slim::last_error(); }
+
+int slimInitDataOnGPU(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    int rc = ensure_device(c);
+    if (rc) return rc;
+    if ((rc = check_scene_arrays(scene))) return rc;
+    c.initialized = false;
+    c.counts = scene->counts;
+    c.geometries.clear();
+    c.materials.clear();
+    if ((rc = upload_materials(c, scene))) return rc;
+    if ((rc = upload_meshes(c, scene))) return rc;
+    if ((rc = upload_textures(c, scene))) return rc;
+    if ((rc = upload_lights(c, scene))) return rc;
+    if ((rc = upload_geometries(c, scene))) return rc;
+    c.scene.geometry_count = c.counts.geometries;
+    c.scene.material_count = c.counts.materials;
+    if ((rc = upload_scene_bvh(c, scene))) return rc;
+    c.initialized = true;
+    return SLIM_OK;
+}
+
+int slimUploadLights(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int rc = require_init(g_ctx, scene);
+    if (rc) return rc;
+    if (scene->counts.lights != g_ctx.counts.lights || (scene->counts.lights && !scene->lights))
+        return set_error(SLIM_ERR_STATE, "light count differs from slimInitDataOnGPU");
+    return upload_lights(g_ctx, scene);
+}
+
+int slimUploadCameras(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int rc = require_init(g_ctx, scene);
+    if (rc) return rc;
+    // Cameras are not read by the trace path (renderOnGPU takes the
+    // projection); the hook exists for call compatibility.
+    if (scene->counts.cameras != g_ctx.counts.cameras) return set_error(SLIM_ERR_STATE, "camera count differs");
+    return SLIM_OK;
+}
+
+int slimUploadGeometries(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int rc = require_init(g_ctx, scene);
+    if (rc) return rc;
+    if (scene->counts.geometries != g_ctx.counts.geometries || !scene->geometries)
+        return set_error(SLIM_ERR_STATE, "geometry count differs from slimInitDataOnGPU");
+    return upload_geometries(g_ctx, scene);
+}
+
+int slimUploadMaterials(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int rc = require_init(g_ctx, scene);
+    if (rc) return rc;
+    if (scene->counts.materials != g_ctx.counts.materials || !scene->materials)
+        return set_error(SLIM_ERR_STATE, "material count differs from slimInitDataOnGPU");
+    return upload_materials(g_ctx, scene);
+}
+
+int slimUploadSceneBVH(const SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int rc = require_init(g_ctx, scene);
+    if (rc) return rc;
+    if (scene->counts.geometries != g_ctx.counts.geometries) return set_error(SLIM_ERR_STATE, "geometry count differs");
+    return upload_scene_bvh(g_ctx, scene);
+}
+
+int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                    const SlimRayTracerSettings *settings) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!canvas || !projection || !settings || !canvas->pixels || !canvas->depths)
+        return set_error(SLIM_ERR_ARGUMENT, "slimRenderOnGPU: null argument");
+    const SlimDimensions &dim = canvas->dimensions;
+    uint32_t stride = dim.stride ? dim.stride : dim.width;
+    size_t wth = (size_t)stride * dim.height;
+    size_t pixel_count = wth * (canvas->antialias == SLIM_AA_SSAA ? 4 : 1);
+    size_t depth_count = wth * (canvas->antialias == SLIM_AA_NONE ? 1 : 4);
+    int rc = c.d_pixels.reserve(pixel_count, "alloc frame");
+    if (rc) return rc;
+    if ((rc = c.d_depths.reserve(depth_count, "alloc depths"))) return rc;
+    if ((rc = render(c, canvas, projection, settings, c.d_pixels.ptr, c.d_depths.ptr, c.stream))) return rc;
+    SLIM_CUDA(cudaMemcpyAsync(canvas->pixels, c.d_pixels.ptr, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, c.stream),
+              "download pixels");
+    SLIM_CUDA(cudaMemcpyAsync(canvas->depths, c.d_depths.ptr, depth_count * sizeof(float), cudaMemcpyDeviceToHost, c.stream),
+              "download depths");
+    if ((rc = read_errors(c, c.stream))) return rc;
+    return read_counters(c, c.stream);
+}
+
+int slimRenderToDevice(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                       const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths, void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!canvas || !projection || !settings || !d_pixels || !d_depths)
+        return set_error(SLIM_ERR_ARGUMENT, "slimRenderToDevice: null argument");
+    int rc = render(c, canvas, projection, settings, (float4 *)d_pixels, (float *)d_depths, (cudaStream_t)stream);
+    if (rc) return rc;
+    if (c.options.count_work) {
+        if ((rc = read_errors(c, (cudaStream_t)stream))) return rc;
+        return read_counters(c, (cudaStream_t)stream);
+    }
+    return SLIM_OK;
+}
+
+int slimTracePrimary(const SlimCameraRayProjection *projection, int width, int height, void *d_geometry_ids,
+                     void *d_primitive_ids, void *d_distances, void *d_from_behind, void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!projection || width <= 0 || height <= 0 || !d_geometry_ids || !d_primitive_ids || !d_distances || !d_from_behind)
+        return set_error(SLIM_ERR_ARGUMENT, "slimTracePrimary: bad argument");
+    cudaError_t e = launch_trace_primary(c.scene, *projection, (uint32_t)width, (uint32_t)height, (int *)d_geometry_ids,
+                                         (uint32_t *)d_primitive_ids, (float *)d_distances, (uint8_t *)d_from_behind,
+                                         c.d_error.ptr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "trace primary launch");
+    return read_errors(c, (cudaStream_t)stream);
+}
+
+int slimSetRenderOptions(const SlimRenderOptions *options) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!options) return set_error(SLIM_ERR_ARGUMENT, "options is null");
+    if (options->engine < 0 || options->engine > 1 || options->ray_cones < 0 || options->ray_cones > 1 ||
+        options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 1024 ||
+        (options->block_size % 32))
+        return set_error(SLIM_ERR_ARGUMENT, "bad render options");
+    g_ctx.options = *options;
+    return SLIM_OK;
+}
+
+int slimGetRenderOptions(SlimRenderOptions *options) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!options) return set_error(SLIM_ERR_ARGUMENT, "options is null");
+    *options = g_ctx.options;
+    return SLIM_OK;
+}
+
+int slimGetWorkCounters(SlimWorkCounters *counters) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!counters) return set_error(SLIM_ERR_ARGUMENT, "counters is null");
+    *counters = g_ctx.last_counters;
+    return SLIM_OK;
+}
+
+int slimRefitSceneBVH(void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    cudaError_t e = launch_refit_scene_bvh(c.scene, c.d_scene_nodes.ptr, c.d_refit_order.ptr,
+                                           (uint32_t)c.refit_order.size(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "refit launch");
+    return SLIM_OK;
+}
+
+int slimProjectionReset(const float orientation9[9], const float position3[3], float focal_length, int width, int height,
+                        int antialias_ssaa, SlimCameraRayProjection *out) {
+    return slim::projection_reset(orientation9, position3, focal_length, width, height, antialias_ssaa, out);
+}
+
+int slimBuildSceneBVH(SlimSceneData *scene) { return slim::build_scene_bvh(scene); }
+
+int slimBuildMesh(float *positions, uint32_t vertex_count, const uint32_t *position_indices, uint32_t triangle_count,
+                  const float *normals, uint32_t normals_count, const uint32_t *normal_indices, const float *uvs,
+                  uint32_t uvs_count, const uint32_t *uv_indices, SlimTriangle *out_triangles, SlimBVHNode *out_nodes,
+                  uint32_t *out_node_count, uint32_t *out_height, float out_aabb6[6]) {
+    return slim::build_mesh(positions, vertex_count, position_indices, triangle_count, normals, normals_count,
+                            normal_indices, uvs, uvs_count, uv_indices, out_triangles, out_nodes, out_node_count,
+                            out_height, out_aabb6);
+}
+
+int slimReadMeshHeader(const char *path, SlimMesh *mesh) { return slim::read_mesh_header(path, mesh); }
+int slimReadMesh(const char *path, SlimMesh *mesh) { return slim::read_mesh(path, mesh); }
+int slimWriteMesh(const char *path, const SlimMesh *mesh) { return slim::write_mesh(path, mesh); }
+int slimReadTextureHeader(const char *path, SlimTexture *texture, uint32_t *total_texel_quads) {
+    return slim::read_texture_header(path, texture, total_texel_quads);
+}
+int slimReadTexture(const char *path, SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *texel_quads) {
+    return slim::read_texture(path, texture, mips, texel_quads);
+}
+int slimWriteTexture(const char *path, const SlimTexture *texture) { return slim::write_texture(path, texture); }
+int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
+                    SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *texel_quads, uint32_t *mip_count,
+                    uint32_t *texel_quad_count) {
+    return slim::bake_texture(bgr, width, height, channels, flags, texture, mips, texel_quads, mip_count, texel_quad_count);
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+// The fused (one thread per sample, whole path in one kernel) form of the
+// trace path, plus the primary-hit kernel used for id/distance parity.
+// Mirrors d_render (renderer/renderer_GPU.h:22-46) -> renderPixel
+// (renderer/ray_tracer.h:19-161).
+#include "kernels.h"
+#include "tracer_core.cuh"
+
+namespace slim {
+namespace dev {
+
+template <bool COUNT>
+SLIM_D void flush_work(const DevFrame &F, const Work &w) {
+    if (!COUNT || !F.counters) return;
+    uint32_t v[9] = {w.primary, w.shadow, w.bounce, w.scene_nodes, w.mesh_nodes, w.triangles,
+                     w.geometries, w.mesh_fetches, w.taps};
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        unsigned long long s = v[k];
+        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(F.counters + k, s);
+    }
+}
+
+// renderPixelBeauty / renderPixelDebugMode for one sample.
+template <bool COUNT>
+SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, uint32_t *stack,
+                          uint32_t *mesh_stack, uint32_t &err, Work &w, float3 &out_color, float &out_depth) {
+    const SlimCameraRayProjection &P = F.projection;
+    const SlimRayTracerSettings &st = F.settings;
+    float scaling = F.cones_per_pixel ? pixel_scaling(P, x, y) : 0.0f;
+    float3 cam = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
+    Ray ray;
+    reset(ray, cam, normalized(primary_direction(P, x, y)));
+    Hit hit;
+    bump<COUNT>(w.primary);
+    float3 color = f3(0, 0, 0);
+    float depth = INFINITY;
+    Surface s;
+    if (st.render_mode != SLIM_RENDER_BEAUTY) {
+        int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+        if (g >= 0) {
+            Geo geo = load_geo(S, (uint32_t)g);
+            Mat m = load_mat(S, geo.material);
+            prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+            depth = depth_at(P, hit.position);
+            switch (st.render_mode) {
+                case SLIM_RENDER_UVS: color = f3(hit.u, hit.v, 1.0f); break;
+                case SLIM_RENDER_DEPTH: { float d = 4.0f / hit.distance; color = f3(d, d, d); } break;
+                case SLIM_RENDER_NORMALS:
+                    color = f3(fmaf(hit.normal.x, 0.5f, 0.5f), fmaf(hit.normal.y, 0.5f, 0.5f), fmaf(hit.normal.z, 0.5f, 0.5f));
+                    break;
+                case SLIM_RENDER_NORMAL_MAP: {
+                    float3 n = sample_slot<COUNT>(S, m, 1, hit.u, hit.v, hit.uv_coverage, w);
+                    color = f3(fmaf(n.x, 0.5f, 0.5f), fmaf(n.y, 0.5f, 0.5f), fmaf(n.z, 0.5f, 0.5f));
+                } break;
+                case SLIM_RENDER_MIP_LEVEL:
+                    if (S.texture_count) {
+                        DevTexture t0 = S.textures[0];
+                        color = color_of_id(st.mip_level_colors[mip_level(hit.uv_coverage * (float)(t0.width * t0.height), t0.mip_count)]);
+                    } else color = f3(0.5f, 0.5f, 0.5f);
+                    break;
+                default: break;
+            }
+        }
+        out_color = color;
+        out_depth = depth;
+        return;
+    }
+    float3 throughput = f3(1, 1, 1), next_throughput = f3(0, 0, 0);
+    uint32_t depth_left = st.max_depth;
+    while (depth_left) {
+        float3 current = f3(0, 0, 0);
+        int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+        if (g >= 0) {
+            Geo geo = load_geo(S, (uint32_t)g);
+            Mat m = load_mat(S, geo.material);
+            if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+                depth_left = 0;
+                current = m.emission;
+            } else {
+                prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+                if (depth_left == st.max_depth) depth = depth_at(P, hit.position);
+                for (uint32_t i = 0; i < S.light_count; i++) {
+                    LightRec l = load_light(S, i);
+                    if (!is_facing_light(s, l)) continue;
+                    if (l.flags & SLIM_LIGHT_IS_SHADOWING) {
+                        Ray sr;
+                        sr.o = s.P;
+                        sr.d = s.L;
+                        Hit sh;
+                        bump<COUNT>(w.shadow);
+                        if (scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0) continue;
+                    }
+                    add_light(s, m, l, current);
+                }
+                if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
+                if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
+                    s.L = s.N;
+                    s.NdotL = 1.0f;
+                    float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
+                    float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
+                    radiance_fraction(s, m);
+                    current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
+                }
+                if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && --depth_left) {
+                    float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
+                    next_throughput = s.refracted ? one_minus(Fr) : Fr;
+                    reset(ray, hit.position, s.RF);
+                    bump<COUNT>(w.bounce);
+                } else depth_left = 0;
+            }
+        } else {
+            depth_left = 0;
+            if (st.skybox_color_texture_id >= 0)
+                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+        }
+        add_glow(S, ray, hit.distance, current);
+        color = mul_add(current, throughput, color);
+        throughput = throughput * next_throughput;
+    }
+    out_color = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
+    out_depth = depth;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    Work w = {};
+    if (i < F.width * F.height) {
+        int x = (int)(i % F.width), y = (int)(i / F.width);
+        uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+        uint32_t err = 0;
+        float3 color;
+        float depth;
+        render_sample<COUNT>(S, F, x, y, stack, mesh_stack, err, w, color, depth);
+        set_pixel(F, x, y, color, depth);
+        if (err) atomicOr(F.error_flags, err);
+    }
+    flush_work<COUNT>(F, w);
+}
+
+// First closest hit of each primary ray (renderer/ray_tracer.h:36-45).
+__global__ void __launch_bounds__(128) k_trace_primary(DevScene S, SlimCameraRayProjection P, uint32_t width,
+                                                       uint32_t height, int *geometry_ids, uint32_t *primitive_ids,
+                                                       float *distances, uint8_t *from_behind, uint32_t *error_flags) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= width * height) return;
+    int x = (int)(i % width), y = (int)(i / width);
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    Ray ray;
+    reset(ray, f3(P.camera_position.x, P.camera_position.y, P.camera_position.z), normalized(primary_direction(P, x, y)));
+    Hit hit;
+    int g = scene_trace<false>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+    geometry_ids[i] = g;
+    bool mesh = false;
+    if (g >= 0) mesh = load_geo(S, (uint32_t)g).type == SLIM_GEOMETRY_MESH;
+    primitive_ids[i] = mesh ? hit.id : 0u;
+    distances[i] = g >= 0 ? hit.distance : INFINITY;
+    from_behind[i] = g >= 0 ? (uint8_t)hit.from_behind : (uint8_t)0;
+    if (err) atomicOr(error_flags, err);
+}
+
+}  // namespace dev
+
+cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream) {
+    uint32_t n = F.width * F.height;
+    if (block <= 0) block = 128;
+    if (block > 128) block = 128;
+    dim3 grid((n + block - 1) / block);
+    if (F.counters) dev::k_render_fused<true><<<grid, block, 0, stream>>>(S, F);
+    else dev::k_render_fused<false><<<grid, block, 0, stream>>>(S, F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjection &P, uint32_t width, uint32_t height,
+                                 int *geometry_ids, uint32_t *primitive_ids, float *distances, uint8_t *from_behind,
+                                 uint32_t *error_flags, cudaStream_t stream) {
+    uint32_t n = width * height;
+    dim3 grid((n + 127) / 128);
+    dev::k_trace_primary<<<grid, 128, 0, stream>>>(S, P, width, height, geometry_ids, primitive_ids, distances,
+                                                  from_behind, error_flags);
+    return cudaGetLastError();
+}
+
+}  // namespace slim

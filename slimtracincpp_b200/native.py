@@ -1,0 +1,111 @@
+"""ctypes binding of libslimtracer_b200.so (the C ABI in include/slimtracer_b200.h).
+
+The library is the only compute path: there is no Python or CPU fallback.
+Loading fails loudly when the in-tree build is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import layout as L
+
+LIB_PATH = Path(__file__).resolve().parent / "_native" / "libslimtracer_b200.so"
+
+SLIM_OK = 0
+ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "LIMIT", 5: "IO", 6: "STACK"}
+
+EXPORTS = [
+    "slimInitDataOnGPU", "slimUploadLights", "slimUploadCameras", "slimUploadGeometries", "slimUploadMaterials",
+    "slimUploadSceneBVH", "slimRenderOnGPU", "slimGetLastError", "slimGetVersion", "slimSetRenderOptions",
+    "slimGetRenderOptions", "slimRenderToDevice", "slimTracePrimary", "slimGetWorkCounters", "slimRefitSceneBVH",
+    "slimProjectionReset", "slimBuildSceneBVH", "slimBuildMesh", "slimReadMeshHeader", "slimReadMesh",
+    "slimWriteMesh", "slimReadTextureHeader", "slimReadTexture", "slimWriteTexture", "slimBakeTexture",
+]
+
+
+class SlimError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"SLIM_ERR_{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+_lib = None
+P = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m slimtracincpp_b200.build` "
+                           "(the trace path has no CPU fallback)")
+    h = C.CDLL(str(LIB_PATH))
+    for name in EXPORTS:
+        getattr(h, name)
+    h.slimGetLastError.restype = C.c_char_p
+    h.slimGetLastError.argtypes = []
+    for name in ["slimInitDataOnGPU", "slimUploadLights", "slimUploadCameras", "slimUploadGeometries",
+                 "slimUploadMaterials", "slimUploadSceneBVH", "slimBuildSceneBVH", "slimSetRenderOptions",
+                 "slimGetRenderOptions", "slimGetWorkCounters", "slimRefitSceneBVH"]:
+        getattr(h, name).argtypes = [P]
+        getattr(h, name).restype = C.c_int
+    h.slimRenderOnGPU.argtypes = [P, P, P]
+    h.slimRenderToDevice.argtypes = [P, P, P, P, P, P]
+    h.slimTracePrimary.argtypes = [P, C.c_int, C.c_int, P, P, P, P, P]
+    h.slimProjectionReset.argtypes = [P, P, C.c_float, C.c_int, C.c_int, C.c_int, P]
+    h.slimBuildMesh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, P, P, P]
+    h.slimReadMeshHeader.argtypes = [C.c_char_p, P]
+    h.slimReadMesh.argtypes = [C.c_char_p, P]
+    h.slimWriteMesh.argtypes = [C.c_char_p, P]
+    h.slimReadTextureHeader.argtypes = [C.c_char_p, P, P]
+    h.slimReadTexture.argtypes = [C.c_char_p, P, P, P]
+    h.slimWriteTexture.argtypes = [C.c_char_p, P]
+    h.slimBakeTexture.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
+    for name in EXPORTS:
+        if name not in ("slimGetLastError",):
+            getattr(h, name).restype = C.c_int
+    _lib = h
+    return h
+
+
+def check(rc):
+    if rc != SLIM_OK:
+        msg = lib().slimGetLastError().decode(errors="replace")
+        raise SlimError(rc, msg)
+    return rc
+
+
+def ptr(a) -> int:
+    """Address of a numpy array (or 0 for None)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a)
+
+
+def projection_reset(orientation9, position3, focal_length, width, height, ssaa=False):
+    """CameraRayProjection::reset (scene/camera.h:69-83)."""
+    out = np.zeros((), L.PROJECTION)
+    o = np.ascontiguousarray(orientation9, dtype=np.float32)
+    p = np.ascontiguousarray(position3, dtype=np.float32)
+    check(lib().slimProjectionReset(ptr(o), ptr(p), C.c_float(focal_length), width, height, int(bool(ssaa)), ptr(out)))
+    return out
+
+
+def set_render_options(engine=L.ENGINE_WAVEFRONT, ray_cones=L.CONES_REFERENCE, scene_bvh=L.SCENE_BVH_UPLOADED,
+                       block_size=0, count_work=False):
+    o = np.zeros((), L.RENDER_OPTIONS)
+    o["engine"], o["ray_cones"], o["scene_bvh"] = engine, ray_cones, scene_bvh
+    o["block_size"], o["count_work"] = block_size, int(bool(count_work))
+    check(lib().slimSetRenderOptions(ptr(o)))
+
+
+def work_counters():
+    w = np.zeros((), L.WORK_COUNTERS)
+    check(lib().slimGetWorkCounters(ptr(w)))
+    return {k: int(w[k]) for k in L.WORK_COUNTERS.names}

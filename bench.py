@@ -1,0 +1,359 @@
+#!/usr/bin/env python3
+"""Throughput of the B200 trace path on the 1080p mesh PBR workload.
+
+Workload (config 2): 1920x1080, bounce depth 2, an icosphere (81,920
+triangles) and a value-noise heightfield (130,050 triangles), 8 instances,
+Cook-Torrance materials, 4 point lights, 1 emissive-quad area light,
+synthetic seeded scene (no dataset).  A step is one frame: GPU refit of the
+scene BVH + the full per-pixel path (primary, shadow and bounce rays, area
+lights, glow, tone mapping, canvas write).
+
+  value  Mrays/s with the scene resident in HBM (device buffers, CUDA events
+         around each frame; L2 flushed between frames by writing 512 MiB).
+  e2e    the same metric through the reference-facing C ABI with host
+         buffers: per step slimUploadGeometries (H2D from pinned memory),
+         slimRefitSceneBVH and slimRenderOnGPU into a pinned host canvas
+         (D2H of pixels + depths).
+
+Mrays/s counts every traced ray (primary + shadow + bounce), as counted by
+the kernels' work counters on one untimed frame.
+
+`--impl reference` times the reference's own CPU renderer (compiled from
+its sources into oracle/_ref) on the host cores with the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s & ms/frame at 1080p: plain GPU vs radiance-cache at ≥40 dB PSNR"
+UNIT = "Mrays/s"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    return p.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def algorithmic_bytes(w):
+    """Bytes the path must touch per frame (memory-hierarchy roofline):
+    32 B per BVH node test, 64 B per triangle test, 64 B per mesh-hit
+    attribute fetch, 72 B per instance test, 16 B per texel-quad tap, plus
+    20 B per sample of framebuffer written."""
+    return (32 * (w["scene_node_tests"] + w["mesh_node_tests"]) + 64 * w["triangle_tests"] +
+            64 * w["mesh_hit_fetches"] + 72 * w["geometry_tests"] + 16 * w["texel_taps"] + 20 * w["primary_rays"])
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(workload, seconds, threads=None):
+    """The reference's own CPU renderer (oracle/_ref) on the host cores, on
+    a bounded sample of the same frame: horizontal bands spread over the
+    image until `seconds` of wall time are spent.  Ray counts of the sample
+    come from the oracle's counters for the same rows."""
+    from oracle import bindings as O
+    from slimtracincpp_b200 import layout as L
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if O.reference_available() else "port"
+    proj = workload.projection()
+    h = workload.height
+    band = max(1, h // 36)
+    starts = list(range(0, h, band))
+    order = starts[::2] + starts[1::2]
+    band_rays = {}
+    rows_done, rays, t_total, frames = 0, 0, 0.0, 0
+    while t_total < seconds:
+        for r0 in order:
+            r1 = min(h, r0 + band)
+            t0 = time.perf_counter()
+            if kind == "reference":
+                O.reference_render(workload.scene, proj, workload.settings, workload.width, workload.height,
+                                   rows=(r0, r1), threads=threads, layout=L)
+            else:
+                O.oracle_render(workload.scene, proj, workload.settings, workload.width, workload.height,
+                                rows=(r0, r1), layout=L)
+            t_total += time.perf_counter() - t0
+            if r0 not in band_rays:
+                _, _, work = O.oracle_render(workload.scene, proj, workload.settings, workload.width, workload.height,
+                                             rows=(r0, r1), layout=L, count=True)
+                band_rays[r0] = work["primary_rays"] + work["shadow_rays"] + work["bounce_rays"]
+            rays += band_rays[r0]
+            rows_done += r1 - r0
+            if t_total >= seconds:
+                break
+        frames += 1
+    cores = threads if kind == "reference" else 1
+    return {"value": rays / t_total / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{rows_done} rows ({rows_done / h:.2f} frames, {rays} rays) of the {workload.width}x"
+                      f"{workload.height} frame rendered in {band}-row bands, {t_total:.2f} s wall on {cores} threads",
+            "seconds": t_total}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    from slimtracincpp_b200 import scenes
+    from oracle import bindings as O
+    w = scenes.config2(args.seed)
+    if not O.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libslimref.so was not built"}))
+        return 0
+    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(w, 0.5)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(w, per_step))
+    wall = time.perf_counter() - t0
+    rays = sum(v["value"] * v["seconds"] for v in vals) * 1e6
+    secs = sum(v["seconds"] for v in vals)
+    value = rays / secs / 1e6
+    frame_rays = None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 scene)",
+            "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 2,
+                       "instances": 8, "triangles": 81920 + 130050, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": vals[0]["kind"],
+                             "sample": vals[0]["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_info()
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200 import native, scenes
+    from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport, make_canvas
+
+    engine = L.ENGINE_WAVEFRONT if args.engine == "wavefront" else L.ENGINE_MEGAKERNEL
+    w = scenes.config2(args.seed)
+    lib = native.lib()
+    r = RayTracingRenderer(w.scene, max_depth=int(w.settings["max_depth"]))
+    vp = Viewport(w.camera, w.width, w.height)
+    n = w.samples
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    # one counted frame: rays per frame and algorithmic bytes per stage
+    native.set_render_options(engine=engine, count_work=True, profile_stages=True)
+    d_pix = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    d_dep = torch.empty(n, dtype=torch.float32, device=dev)
+    native.check(lib.slimRefitSceneBVH(sp))
+    r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
+    torch.cuda.synchronize()
+    work = native.work_counters()
+    stage_work = {s["name"]: s["work"] for s in native.stage_stats()}
+    rays_per_frame = work["primary_rays"] + work["shadow_rays"] + work["bounce_rays"]
+
+    # timed device-resident frames
+    native.set_render_options(engine=engine, profile_stages=True)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
+    torch.cuda.synchronize()
+    native.reset_stage_stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    stats = {s["name"]: s for s in native.stage_stats()}
+
+    # end to end through the C ABI with host buffers
+    native.set_render_options(engine=engine)
+    pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    pin_geo = torch.empty(w.scene.geometries.nbytes, dtype=torch.uint8, pin_memory=True)
+    host_geo = pin_geo.numpy().view(L.GEOMETRY)
+    host_geo[:] = w.scene.geometries
+    sd = w.scene.data.copy()
+    sd["geometries"] = pin_geo.data_ptr()
+    cv, _, _ = make_canvas(w.width, w.height, L.AA_NONE)
+    cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
+    proj = w.projection()
+    for _ in range(args.warmup):
+        native.check(lib.slimUploadGeometries(native.ptr(sd)))
+        native.check(lib.slimRefitSceneBVH(None))
+        native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        native.check(lib.slimUploadGeometries(native.ptr(sd)))
+        native.check(lib.slimRefitSceneBVH(None))
+        native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
+    e2e_s = time.perf_counter() - t0
+    h2d = int(w.scene.geometries.nbytes)
+    d2h = int(pin_pix.numel() * 4 + pin_dep.numel() * 4)
+
+    # max over ranks
+    times = torch.tensor([total_ms, e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    total_ms, e2e_s = float(times[0]), float(times[1])
+    value = rays_per_frame * args.steps * world / (total_ms / 1000.0) / 1e6
+    e2e_value = rays_per_frame * args.steps * world / e2e_s / 1e6
+
+    # roofline of the dominant kernel
+    timed = {k: v for k, v in stats.items() if v["launches"]}
+    dom_name = max(timed, key=lambda k: timed[k]["total_ms"]) if timed else None
+    peak, peak_kind = measured_peaks()
+    roofline = None
+    if dom_name:
+        d = timed[dom_name]
+        per_launch_ms = d["total_ms"] / d["launches"]
+        launches_per_frame = d["launches"] / args.steps
+        alg = algorithmic_bytes(stage_work[dom_name]) / max(1.0, launches_per_frame)
+        achieved = alg / (per_launch_ms / 1000.0) / 1e9
+        roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "traffic": None, "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
+                    "share_of_frame": d["total_ms"] / total_ms}
+    frame_bytes = algorithmic_bytes(work)
+    # kernels of this library in the timed region (refit = leaves + inner kernels)
+    launches = sum(v["launches"] * (2 if k == "refit" else 1) for k, v in stats.items())
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 scene)",
+            "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 2, "instances": 8,
+                       "triangles": 81920 + 130050, "engine": args.engine, "parallelism": f"replicas x{world}",
+                       "l2": "flushed between steps (512 MiB write)", "rays_per_frame": rays_per_frame,
+                       "primary_rays": work["primary_rays"], "shadow_rays": work["shadow_rays"],
+                       "bounce_rays": work["bounce_rays"]},
+            "ms_per_frame": total_ms / args.steps,
+            "frame_algorithmic_bytes": frame_bytes,
+            "frame_achieved_gbs": frame_bytes / (total_ms / args.steps / 1000.0) / 1e9,
+            "roofline": roofline,
+            "stages_ms_per_frame": {k: v["total_ms"] / args.steps for k, v in timed.items()},
+            "stage_work_per_frame": {k: v for k, v in stage_work.items() if any(v.values())},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1000.0 * e2e_s / args.steps},
+            "clocks": clock_info,
+            "gpu_launches": launches}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = {k: v for k, v in cpu_baseline(w, args.cpu_seconds).items() if k != "seconds"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

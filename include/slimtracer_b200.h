@@ -190,7 +190,9 @@ typedef struct {
     int32_t scene_bvh;       /* SLIM_SCENE_BVH_UPLOADED (default) or GPU refit of its topology */
     int32_t block_size;      /* threads per block, 0 = tuned default */
     int32_t count_work;      /* non-zero: accumulate per-frame work counters (slower) */
-    int32_t _reserved[3];
+    int32_t profile_stages;  /* non-zero: time every stage launch with CUDA events */
+    int32_t shadow_queue_mb; /* wavefront shadow-ray queue budget in MiB, 0 = 1024 */
+    int32_t _reserved;
 } SlimRenderOptions;
 
 /* Work counters of the last frame (rays traced and memory records touched). */
@@ -276,6 +278,19 @@ int slimTracePrimary(const SlimCameraRayProjection *projection, int width, int h
 
 /* Work counters of the last frame rendered with options.count_work set. */
 int slimGetWorkCounters(SlimWorkCounters *counters);
+
+/* Per-stage launch statistics accumulated while options.profile_stages is
+ * set (stage names: fused, extend, shadow_gen, shadow, shade, refit):
+ * launches, summed CUDA-event milliseconds and -- with count_work -- the
+ * work counters of the last frame.  Fills up to `capacity` entries. */
+typedef struct {
+    char name[24];
+    uint32_t launches;
+    float total_ms;
+    SlimWorkCounters work;
+} SlimStageStats;
+int slimGetStageStats(SlimStageStats *stats, int capacity, int *count);
+int slimResetStageStats(void);
 
 /* Re-fits the device copy of the scene BVH to the current geometries
  * (GPU), keeping the topology last uploaded: scene/scene.h:165-191 rebuilds

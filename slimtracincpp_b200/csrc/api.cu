@@ -79,9 +79,56 @@ struct Context {
     SlimRenderOptions options{};
     SlimWorkCounters last_counters{};
     WavefrontBuffers wavefront{};
-    DevArray<float4> w_color, w_through, w_next, w_rays0, w_rays1, w_hits, w_shadow_rays;
-    DevArray<uint32_t> w_counts, w_shadow_meta, w_shadow_mask;
+    DevArray<float4> w_color, w_through, w_rays0, w_rays1, w_hits, w_shadow_rays;
+    DevArray<uint32_t> w_counts;
+    DevArray<unsigned long long> w_shadow_mask;
+    struct EventTimer *timer = nullptr;
 };
+
+// CUDA-event pairs around stage launches, resolved lazily.
+struct EventTimer : StageTimer {
+    struct Pending { int stage; cudaEvent_t a, b; };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Pending> pending;
+    cudaEvent_t open[STAGE_COUNT] = {};
+    uint32_t launches[STAGE_COUNT] = {};
+    double total_ms[STAGE_COUNT] = {};
+    cudaEvent_t take() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int stage, cudaStream_t stream) override {
+        cudaEvent_t e = take();
+        cudaEventRecord(e, stream);
+        open[stage] = e;
+    }
+    void end(int stage, cudaStream_t stream) override {
+        cudaEvent_t e = take();
+        cudaEventRecord(e, stream);
+        pending.push_back({stage, open[stage], e});
+        open[stage] = nullptr;
+    }
+    void resolve() {
+        for (auto &p : pending) {
+            cudaEventSynchronize(p.b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            launches[p.stage]++;
+            total_ms[p.stage] += ms;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        resolve();
+        for (int i = 0; i < STAGE_COUNT; i++) { launches[i] = 0; total_ms[i] = 0; }
+    }
+};
+const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit"};
+SlimWorkCounters g_stage_work[STAGE_COUNT];
 
 Context g_ctx;
 std::mutex g_mutex;
@@ -96,7 +143,7 @@ int ensure_device(Context &c) {
     SLIM_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     int rc = c.d_error.reserve(1, "alloc error flags");
     if (rc) return rc;
-    rc = c.d_counters.reserve(16, "alloc counters");
+    rc = c.d_counters.reserve(kCountersPerStage * STAGE_COUNT, "alloc counters");
     if (rc) return rc;
     SLIM_CUDA(cudaMemset(c.d_error.ptr, 0, sizeof(uint32_t)), "clear error flags");
     return SLIM_OK;
@@ -426,6 +473,12 @@ int check_settings(const Context &c, const SlimRayTracerSettings *st) {
 
 int ensure_wavefront(Context &c, uint32_t samples);
 
+StageTimer *timer_for(Context &c) {
+    if (!c.options.profile_stages) return nullptr;
+    if (!c.timer) c.timer = new EventTimer();
+    return c.timer;
+}
+
 int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
            const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream) {
     const SlimDimensions &dim = canvas->dimensions;
@@ -448,46 +501,52 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     F.depths = d_depths;
     F.error_flags = c.d_error.ptr;
     F.counters = c.options.count_work ? c.d_counters.ptr : nullptr;
-    if (F.counters) SLIM_CUDA(cudaMemsetAsync(F.counters, 0, 16 * sizeof(unsigned long long), stream), "clear counters");
+    if (F.counters)
+        SLIM_CUDA(cudaMemsetAsync(F.counters, 0, kCountersPerStage * STAGE_COUNT * sizeof(unsigned long long), stream),
+                  "clear counters");
+    StageTimer *timer = timer_for(c);
     cudaError_t e;
     if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) {
-        e = launch_render_fused(c.scene, F, c.options.block_size, stream);
+        e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer);
     } else {
         rc = ensure_wavefront(c, F.width * F.height);
         if (rc) return rc;
-        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream);
+        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream, timer);
     }
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return SLIM_OK;
 }
 
 int ensure_wavefront(Context &c, uint32_t samples) {
-    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= samples) return SLIM_OK;
+    size_t lights = c.scene.light_count ? c.scene.light_count : 1;
+    size_t budget = (size_t)(c.options.shadow_queue_mb > 0 ? c.options.shadow_queue_mb : 1024) << 20;
+    size_t shadow = (size_t)samples * lights;
+    size_t max_shadow = budget / (2 * sizeof(float4));
+    if (shadow > max_shadow) shadow = max_shadow < samples ? samples : max_shadow;
+    if (shadow > 0xFFFFFFFFull) shadow = 0xFFFFFFFFull;
+    if ((uint64_t)samples << 6 > 0xFFFFFFFFull) return set_error(SLIM_ERR_LIMIT, "frame too large for the wavefront queues");
+    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= shadow) return SLIM_OK;
     uint32_t n = samples;
     int rc = 0;
-    if ((rc = c.w_color.reserve(n, "alloc path color"))) return rc;
+    if ((rc = c.w_color.reserve(n, "alloc path colour"))) return rc;
     if ((rc = c.w_through.reserve(n, "alloc path throughput"))) return rc;
-    if ((rc = c.w_next.reserve(n, "alloc path next throughput"))) return rc;
     if ((rc = c.w_rays0.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
     if ((rc = c.w_rays1.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
-    if ((rc = c.w_hits.reserve(4 * (size_t)n, "alloc hit records"))) return rc;
-    if ((rc = c.w_shadow_rays.reserve(2 * (size_t)n, "alloc shadow queue"))) return rc;
+    if ((rc = c.w_hits.reserve(3 * (size_t)n, "alloc hit records"))) return rc;
+    if ((rc = c.w_shadow_rays.reserve(2 * shadow, "alloc shadow queue"))) return rc;
     if ((rc = c.w_counts.reserve(8, "alloc queue counters"))) return rc;
-    if ((rc = c.w_shadow_meta.reserve(n, "alloc shadow queue"))) return rc;
     if ((rc = c.w_shadow_mask.reserve(n, "alloc shadow masks"))) return rc;
     WavefrontBuffers &B = c.wavefront;
     B.path_color = c.w_color.ptr;
     B.path_throughput = c.w_through.ptr;
-    B.path_next = c.w_next.ptr;
     B.rays[0] = c.w_rays0.ptr;
     B.rays[1] = c.w_rays1.ptr;
     B.queue_count = c.w_counts.ptr;
     B.hits = c.w_hits.ptr;
     B.shadow_rays = c.w_shadow_rays.ptr;
-    B.shadow_meta = c.w_shadow_meta.ptr;
     B.shadow_mask = c.w_shadow_mask.ptr;
     B.capacity = n;
-    B.shadow_capacity = n;
+    B.shadow_capacity = (uint32_t)shadow;
     return SLIM_OK;
 }
 
@@ -505,14 +564,23 @@ int read_errors(Context &c, cudaStream_t stream) {
 
 int read_counters(Context &c, cudaStream_t stream) {
     if (!c.options.count_work) return SLIM_OK;
-    unsigned long long v[16];
+    unsigned long long v[kCountersPerStage * STAGE_COUNT];
     SLIM_CUDA(cudaMemcpyAsync(v, c.d_counters.ptr, sizeof(v), cudaMemcpyDeviceToHost, stream), "read counters");
     SLIM_CUDA(cudaStreamSynchronize(stream), "read counters");
     SlimWorkCounters &w = c.last_counters;
-    w.primary_rays = v[0]; w.shadow_rays = v[1]; w.bounce_rays = v[2];
-    w.scene_node_tests = v[3]; w.mesh_node_tests = v[4]; w.triangle_tests = v[5];
-    w.geometry_tests = v[6]; w.mesh_hit_fetches = v[7]; w.texel_taps = v[8];
-    w.pixels = v[0];
+    memset(&w, 0, sizeof(w));
+    for (int st = 0; st < STAGE_COUNT; st++) {
+        const unsigned long long *p = v + kCountersPerStage * st;
+        SlimWorkCounters &sw = g_stage_work[st];
+        sw.primary_rays = p[0]; sw.shadow_rays = p[1]; sw.bounce_rays = p[2];
+        sw.scene_node_tests = p[3]; sw.mesh_node_tests = p[4]; sw.triangle_tests = p[5];
+        sw.geometry_tests = p[6]; sw.mesh_hit_fetches = p[7]; sw.texel_taps = p[8];
+        sw.pixels = 0;
+        w.primary_rays += p[0]; w.shadow_rays += p[1]; w.bounce_rays += p[2];
+        w.scene_node_tests += p[3]; w.mesh_node_tests += p[4]; w.triangle_tests += p[5];
+        w.geometry_tests += p[6]; w.mesh_hit_fetches += p[7]; w.texel_taps += p[8];
+    }
+    w.pixels = w.primary_rays;
     return SLIM_OK;
 }
 
@@ -677,8 +745,35 @@ int slimRefitSceneBVH(void *stream) {
     Context &c = g_ctx;
     if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
     cudaError_t e = launch_refit_scene_bvh(c.scene, c.d_scene_nodes.ptr, c.d_refit_order.ptr,
-                                           (uint32_t)c.refit_order.size(), (cudaStream_t)stream);
+                                           (uint32_t)c.refit_order.size(), (cudaStream_t)stream, timer_for(c));
     if (e != cudaSuccess) return cuda_fail(e, "refit launch");
+    return SLIM_OK;
+}
+
+int slimGetStageStats(SlimStageStats *stats, int capacity, int *count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!stats || capacity < 0 || !count) return set_error(SLIM_ERR_ARGUMENT, "slimGetStageStats: bad argument");
+    Context &c = g_ctx;
+    if (c.timer) c.timer->resolve();
+    int n = 0;
+    for (int st = 0; st < STAGE_COUNT && n < capacity; st++) {
+        SlimStageStats &o = stats[n++];
+        memset(&o, 0, sizeof(o));
+        strncpy(o.name, kStageNames[st], sizeof(o.name) - 1);
+        if (c.timer) {
+            o.launches = c.timer->launches[st];
+            o.total_ms = (float)c.timer->total_ms[st];
+        }
+        o.work = g_stage_work[st];
+    }
+    *count = n;
+    return SLIM_OK;
+}
+
+int slimResetStageStats(void) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (g_ctx.timer) g_ctx.timer->reset();
+    memset(g_stage_work, 0, sizeof(g_stage_work));
     return SLIM_OK;
 }
 

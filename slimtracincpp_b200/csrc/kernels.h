@@ -5,8 +5,21 @@
 
 namespace slim {
 
+// Stages of a frame, for per-stage timing and work counters (16 counter
+// slots per stage in DevFrame::counters).
+enum Stage : int { STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_COUNT };
+constexpr int kCountersPerStage = 16;
+
+// Optional CUDA-event timing around each stage launch.
+struct StageTimer {
+    virtual void begin(int stage, cudaStream_t stream) = 0;
+    virtual void end(int stage, cudaStream_t stream) = 0;
+    virtual ~StageTimer() = default;
+};
+
 // One thread per sample, the whole path in one kernel.
-cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream);
+cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
+                                StageTimer *timer);
 
 // First closest hit of every primary ray.
 cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjection &P, uint32_t width, uint32_t height,
@@ -15,28 +28,22 @@ cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjectio
 
 // Wavefront form: stage kernels over compacted ray queues.
 struct WavefrontBuffers {
-    // path state, one slot per sample
-    float4 *path_color;        // accumulated color (xyz) | depth (w)
-    float4 *path_throughput;   // throughput (xyz) | next throughput .x packed later
-    float4 *path_next;         // next throughput (xyz)
-    // ray queues (ping-pong): origin.xyz|pixel, direction.xyz|flags
-    float4 *rays[2];
-    uint32_t *queue_count;     // [0..1] ray queue sizes, [2] shadow queue size
-    // per-ray hit records
-    float4 *hits;              // 4 float4 per ray slot
-    // shadow rays: origin.xyz|ray slot, direction.xyz|max distance
-    float4 *shadow_rays;
-    uint32_t *shadow_meta;     // (ray slot << 8) | light index
-    uint32_t *shadow_mask;     // per ray slot: bit i set = light i occluded
-    uint32_t capacity;         // samples
-    uint32_t shadow_capacity;  // shadow ray slots
+    float4 *path_color;              // per sample: accumulated colour (xyz), depth (w)
+    float4 *path_throughput;         // per sample: throughput (xyz)
+    float4 *rays[2];                 // ping-pong ray queues, 2 float4 per ray
+    uint32_t *queue_count;           // [0..1] ray queue lengths, [2] shadow queue length
+    float4 *hits;                    // 3 float4 per queue slot
+    float4 *shadow_rays;             // 2 float4 per shadow ray
+    unsigned long long *shadow_mask; // per queue slot: occluded-light bits
+    uint32_t capacity;               // samples
+    uint32_t shadow_capacity;        // shadow ray slots
 };
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream);
+                                    cudaStream_t stream, StageTimer *timer);
 
 // GPU refit of the scene BVH: recomputes every node's bounds bottom-up from
 // the geometries' world AABBs, keeping the uploaded topology.
 cudaError_t launch_refit_scene_bvh(const DevScene &S, float4 *scene_nodes, const uint32_t *parent_order,
-                                   uint32_t node_count, cudaStream_t stream);
+                                   uint32_t node_count, cudaStream_t stream, StageTimer *timer);
 
 }  // namespace slim

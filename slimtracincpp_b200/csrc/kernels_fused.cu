@@ -164,13 +164,16 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene S, SlimCameraRay
 
 }  // namespace dev
 
-cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream) {
+cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
+                                StageTimer *timer) {
     uint32_t n = F.width * F.height;
     if (block <= 0) block = 128;
     if (block > 128) block = 128;
     dim3 grid((n + block - 1) / block);
+    if (timer) timer->begin(STAGE_FUSED, stream);
     if (F.counters) dev::k_render_fused<true><<<grid, block, 0, stream>>>(S, F);
     else dev::k_render_fused<false><<<grid, block, 0, stream>>>(S, F);
+    if (timer) timer->end(STAGE_FUSED, stream);
     return cudaGetLastError();
 }
 

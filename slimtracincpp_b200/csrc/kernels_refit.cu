@@ -74,11 +74,13 @@ __global__ void k_refit_inner(float4 *nodes, const uint32_t *order, uint32_t cou
 }  // namespace dev
 
 cudaError_t launch_refit_scene_bvh(const DevScene &S, float4 *scene_nodes, const uint32_t *order, uint32_t inner_count,
-                                   cudaStream_t stream) {
+                                   cudaStream_t stream, StageTimer *timer) {
     uint32_t n = S.scene_node_count;
     if (!n) return cudaSuccess;
+    if (timer) timer->begin(STAGE_REFIT, stream);
     dev::k_refit_leaves<<<(n + 127) / 128, 128, 0, stream>>>(S, scene_nodes, n);
     if (inner_count) dev::k_refit_inner<<<1, 1, 0, stream>>>(scene_nodes, order, inner_count);
+    if (timer) timer->end(STAGE_REFIT, stream);
     return cudaGetLastError();
 }
 

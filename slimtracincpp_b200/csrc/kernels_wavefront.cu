@@ -1,12 +1,384 @@
-// Wavefront form of the trace path (stage kernels over compacted queues).
+// Wavefront form of the trace path.
+//
+// The reference traces each pixel's whole path in one thread
+// (renderer/renderer_GPU.h:22-46 -> renderer/ray_tracer.h:19-108).  Here a
+// frame is a sequence of stage kernels over queues in HBM, one round per
+// bounce:
+//
+//   extend      closest hit of every queued ray  -> hit record      (scene/scene_tracer.h:26-98)
+//   shadow_gen  shading frame of every hit, one shadow ray per facing
+//               shadowing light -> shadow queue                      (surface_shader.h:49-59,147-160)
+//   shadow      any-hit test of every shadow ray -> per-path occlusion bits
+//   shade       full shading with the occlusion bits, area lights, IBL,
+//               glow, throughput; reflective/refractive hits append the
+//               next bounce ray to the next queue; finished paths are tone
+//               mapped and written to the canvas                    (ray_tracer.h:42-107)
+//
+// Each trace stage keeps only traversal state live, so it runs at a much
+// higher occupancy than the fused kernel.  Queues are appended with one
+// atomic per warp (ballot + popc prefix).  Shading applies the lights in
+// the reference's order from the occlusion bits, so every colour is summed
+// in the same order as the reference's per-pixel loop.
 #include "kernels.h"
 #include "tracer_core.cuh"
 
 namespace slim {
+namespace dev {
+
+// Queue records.
+//   ray:    float4 (origin.xyz, pixel)     float4 (direction.xyz, 0)
+//   hit:    float4 (normal.xyz, distance)  float4 (u, v, uv_coverage, NdotRd)
+//           float4 (geometry, from_behind, triangle id, 0)   -- ints as bits
+//   shadow: float4 (origin.xyz, slot<<6 | light)  float4 (direction.xyz, max distance)
+
+SLIM_D uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated queue append: one atomicAdd per warp, slots handed out
+// by the ballot's prefix popcount.  Returns the slot of a thread whose
+// `want` is set.
+SLIM_D uint32_t warp_append(uint32_t *counter, bool want) {
+    uint32_t active = __activemask();
+    uint32_t ballot = __ballot_sync(active, want);
+    uint32_t base = 0;
+    if (ballot) {
+        int leader = __ffs(ballot) - 1;
+        if ((int)lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(ballot));
+        base = __shfl_sync(active, base, leader);
+    }
+    return base + (uint32_t)__popc(ballot & ((1u << lane_id()) - 1u));
+}
+
+SLIM_D void store_hit(float4 *hits, uint32_t slot, int g, const Hit &h) {
+    float4 *p = hits + 3 * (size_t)slot;
+    p[0] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.distance);
+    p[1] = make_float4(h.u, h.v, h.uv_coverage, h.NdotRd);
+    p[2] = make_float4(__int_as_float(g), __uint_as_float((uint32_t)h.from_behind), __uint_as_float(h.id), 0.0f);
+}
+SLIM_D int load_hit(const float4 *hits, uint32_t slot, Hit &h) {
+    const float4 *p = hits + 3 * (size_t)slot;
+    float4 a = p[0], b = p[1], c = p[2];
+    h.normal = xyz(a);
+    h.distance = a.w;
+    h.u = b.x; h.v = b.y; h.uv_coverage = b.z; h.NdotRd = b.w;
+    h.from_behind = __float_as_uint(c.y) != 0;
+    h.id = __float_as_uint(c.z);
+    return __float_as_int(c.x);
+}
+
+template <bool COUNT>
+SLIM_D void flush_stage(unsigned long long *counters, const Work &w) {
+    if (!COUNT || !counters) return;
+    uint32_t v[9] = {w.primary, w.shadow, w.bounce, w.scene_nodes, w.mesh_nodes, w.triangles, w.geometries,
+                     w.mesh_fetches, w.taps};
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        unsigned long long s = v[k];
+        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
+        if (lane_id() == 0 && s) atomicAdd(counters + k, s);
+    }
+}
+
+struct QueueArgs {
+    const float4 *rays_in;        // null: primary rays generated from the slot (= sample index)
+    float4 *rays_out;
+    const uint32_t *count_in;     // null: count = samples
+    uint32_t *count_out;
+    float4 *hits;
+    float4 *shadow_rays;
+    uint32_t *shadow_count;
+    unsigned long long *masks;    // per slot: bit i = light i occluded
+    float4 *path_color;           // per sample: colour, depth
+    float4 *path_throughput;      // per sample: throughput
+    uint32_t samples;
+    uint32_t depth;               // 1-based bounce of this round
+    uint32_t light_begin, light_end;
+    unsigned long long *counters; // this stage's counter slots, or null
+};
+
+SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
+    int x = (int)(i % F.width), y = (int)(i / F.width);
+    const SlimCameraRayProjection &P = F.projection;
+    o = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
+    d = normalized(primary_direction(P, x, y));
+}
+
+SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel) {
+    if (!A.rays_in) {
+        pixel = slot;
+        primary_ray(F, slot, o, d);
+        return;
+    }
+    float4 a = A.rays_in[2 * (size_t)slot], b = A.rays_in[2 * (size_t)slot + 1];
+    o = xyz(a);
+    pixel = __float_as_uint(a.w);
+    d = xyz(b);
+}
+
+SLIM_D uint32_t queue_size(const QueueArgs &A) { return A.count_in ? *A.count_in : A.samples; }
+
+// ---- extend: closest hit of every queued ray ----------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_extend(DevScene S, DevFrame F, QueueArgs A) {
+    uint32_t n = queue_size(A);
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        float3 o, d;
+        uint32_t pixel;
+        load_ray(F, A, slot, o, d, pixel);
+        if (!A.rays_in) bump<COUNT>(w.primary);
+        Ray ray;
+        reset(ray, o, d);
+        Hit hit;
+        int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+        store_hit(A.hits, slot, g, hit);
+    }
+    if (err) atomicOr(F.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// ---- shadow_gen: one shadow ray per facing, shadowing light -------------
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, QueueArgs A) {
+    uint32_t n = queue_size(A);
+    Work w = {};
+    uint32_t stride = gridDim.x * blockDim.x;
+    // Every thread of a warp runs the same number of iterations so the
+    // queue appends stay warp-uniform.
+    uint32_t rounds = (n + stride - 1) / stride;
+    for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
+        bool live = slot < n;
+        Surface s;
+        bool shaded = false;
+        if (live) {
+            if (A.light_begin == 0) A.masks[slot] = 0ull;
+            float3 o, d;
+            uint32_t pixel;
+            load_ray(F, A, slot, o, d, pixel);
+            Hit hit;
+            int g = load_hit(A.hits, slot, hit);
+            if (g >= 0) {
+                Geo geo = load_geo(S, (uint32_t)g);
+                Mat m = load_mat(S, geo.material);
+                if (!((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind)) {
+                    Ray ray;
+                    reset(ray, scale_add(d, kTraceOffset, o), d);
+                    float scaling = F.cones_per_pixel ? pixel_scaling(F.projection, (int)(pixel % F.width), (int)(pixel / F.width)) : 0.0f;
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+                    shaded = true;
+                }
+            }
+        }
+        for (uint32_t li = A.light_begin; li < A.light_end; li++) {
+            bool want = false;
+            if (shaded) {
+                LightRec l = load_light(S, li);
+                want = is_facing_light(s, l) && (l.flags & SLIM_LIGHT_IS_SHADOWING);
+            }
+            uint32_t q = warp_append(A.shadow_count, want);
+            if (want) {
+                bump<COUNT>(w.shadow);
+                A.shadow_rays[2 * (size_t)q] = make_float4(s.P.x, s.P.y, s.P.z, __uint_as_float((slot << 6) | li));
+                A.shadow_rays[2 * (size_t)q + 1] = make_float4(s.L.x, s.L.y, s.L.z, s.Ld);
+            }
+        }
+    }
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// ---- shadow: any-hit tests ------------------------------------------------
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow(DevScene S, DevFrame F, QueueArgs A) {
+    uint32_t n = *A.shadow_count;
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        float4 a = A.shadow_rays[2 * (size_t)q], b = A.shadow_rays[2 * (size_t)q + 1];
+        Ray ray;
+        ray.o = xyz(a);
+        ray.d = xyz(b);
+        Hit hit;
+        if (scene_trace<COUNT>(S, ray, hit, true, b.w, stack, mesh_stack, err, w) >= 0) {
+            uint32_t tag = __float_as_uint(a.w);
+            atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
+        }
+    }
+    if (err) atomicOr(F.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// ---- shade: colour of this segment, next bounce, finished paths --------
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs A) {
+    uint32_t n = queue_size(A);
+    const SlimRayTracerSettings &st = F.settings;
+    Work w = {};
+    uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t rounds = (n + stride - 1) / stride;
+    for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
+        bool live = slot < n;
+        bool bounce = false;
+        uint32_t pixel = 0;
+        float3 bo = f3(0, 0, 0), bd = f3(0, 0, 0);
+        if (live) {
+            float3 o, d;
+            load_ray(F, A, slot, o, d, pixel);
+            Ray ray;
+            reset(ray, scale_add(d, kTraceOffset, o), d);
+            Hit hit;
+            int g = load_hit(A.hits, slot, hit);
+            float4 pc = A.depth == 1 ? make_float4(0, 0, 0, INFINITY) : A.path_color[pixel];
+            float3 color = xyz(pc), throughput = A.depth == 1 ? f3(1, 1, 1) : xyz(A.path_throughput[pixel]);
+            float depth = pc.w;
+            float3 current = f3(0, 0, 0), next_throughput = f3(0, 0, 0);
+            float hit_distance = INFINITY;
+            if (g >= 0) {
+                hit_distance = hit.distance;
+                Geo geo = load_geo(S, (uint32_t)g);
+                Mat m = load_mat(S, geo.material);
+                if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+                    current = m.emission;
+                } else {
+                    Surface s;
+                    float scaling = F.cones_per_pixel ? pixel_scaling(F.projection, (int)(pixel % F.width), (int)(pixel / F.width)) : 0.0f;
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+                    hit_distance = hit.distance;
+                    if (A.depth == 1) depth = depth_at(F.projection, hit.position);
+                    unsigned long long occluded = A.masks[slot];
+                    for (uint32_t i = 0; i < S.light_count; i++) {
+                        LightRec l = load_light(S, i);
+                        if (!is_facing_light(s, l)) continue;
+                        if ((l.flags & SLIM_LIGHT_IS_SHADOWING) && ((occluded >> i) & 1ull)) continue;
+                        add_light(s, m, l, current);
+                    }
+                    if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
+                    if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
+                        s.L = s.N;
+                        s.NdotL = 1.0f;
+                        float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
+                        float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
+                        radiance_fraction(s, m);
+                        current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
+                    }
+                    if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && A.depth < st.max_depth) {
+                        float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
+                        next_throughput = s.refracted ? one_minus(Fr) : Fr;
+                        bounce = true;
+                        bo = hit.position;
+                        bd = s.RF;
+                        reset(ray, bo, bd);
+                    }
+                }
+            } else if (st.skybox_color_texture_id >= 0) {
+                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+            }
+            add_glow(S, ray, hit_distance, current);
+            color = mul_add(current, throughput, color);
+            throughput = throughput * next_throughput;
+            if (bounce) {
+                A.path_color[pixel] = make_float4(color.x, color.y, color.z, depth);
+                A.path_throughput[pixel] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+            } else {
+                float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
+                set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, depth);
+            }
+        }
+        uint32_t q = warp_append(A.count_out, bounce);
+        if (bounce) {
+            bump<COUNT>(w.bounce);
+            A.rays_out[2 * (size_t)q] = make_float4(bo.x, bo.y, bo.z, __uint_as_float(pixel));
+            A.rays_out[2 * (size_t)q + 1] = make_float4(bd.x, bd.y, bd.z, 0.0f);
+        }
+    }
+    flush_stage<COUNT>(A.counters, w);
+}
+
+template <bool COUNT>
+cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block, cudaStream_t stream,
+                      StageTimer *timer) {
+    uint32_t samples = F.width * F.height;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (block <= 0) block = 256;
+    // Persistent-style grids: enough resident blocks to fill every SM, the
+    // threads stride over the device-side queue length.
+    auto grid_for = [&](const void *kernel, uint32_t work) {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+        uint32_t g = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
+        uint32_t need = (work + block - 1) / block;
+        return need < g ? (need ? need : 1) : g;
+    };
+    uint32_t lights = S.light_count;
+    unsigned long long *C = F.counters;
+    auto stage_counters = [&](int stage) { return C ? C + kCountersPerStage * stage : nullptr; };
+    cudaError_t e = cudaMemsetAsync(B.queue_count, 0, 8 * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    QueueArgs A{};
+    A.hits = B.hits;
+    A.shadow_rays = B.shadow_rays;
+    A.masks = B.shadow_mask;
+    A.path_color = B.path_color;
+    A.path_throughput = B.path_throughput;
+    A.samples = samples;
+    uint32_t max_depth = F.settings.max_depth;
+    for (uint32_t depth = 1; depth <= max_depth; depth++) {
+        uint32_t in = (depth - 1) & 1, out = depth & 1;
+        A.depth = depth;
+        A.rays_in = depth == 1 ? nullptr : B.rays[in];
+        A.count_in = depth == 1 ? nullptr : B.queue_count + in;
+        A.rays_out = B.rays[out];
+        A.count_out = B.queue_count + out;
+        // the output queue of this round is the input of the next: clear it
+        if (depth > 1) {
+            e = cudaMemsetAsync(B.queue_count + out, 0, sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+        }
+        uint32_t bound = depth == 1 ? samples : samples;   // queue length is at most one ray per sample
+        A.counters = stage_counters(STAGE_EXTEND);
+        if (timer) timer->begin(STAGE_EXTEND, stream);
+        k_extend<COUNT><<<grid_for((const void *)k_extend<COUNT>, bound), block, 0, stream>>>(S, F, A);
+        if (timer) timer->end(STAGE_EXTEND, stream);
+        // Shadow rays in light batches that fit the shadow queue.
+        uint32_t per_batch = B.shadow_capacity / (samples ? samples : 1);
+        if (per_batch < 1) per_batch = 1;
+        for (uint32_t l0 = 0; l0 < lights; l0 += per_batch) {
+            A.light_begin = l0;
+            A.light_end = l0 + per_batch < lights ? l0 + per_batch : lights;
+            e = cudaMemsetAsync(B.queue_count + 2, 0, sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
+            A.shadow_count = B.queue_count + 2;
+            A.counters = stage_counters(STAGE_SHADOW_GEN);
+            if (timer) timer->begin(STAGE_SHADOW_GEN, stream);
+            k_shadow_gen<COUNT><<<grid_for((const void *)k_shadow_gen<COUNT>, bound), block, 0, stream>>>(S, F, A);
+            if (timer) timer->end(STAGE_SHADOW_GEN, stream);
+            A.counters = stage_counters(STAGE_SHADOW);
+            if (timer) timer->begin(STAGE_SHADOW, stream);
+            k_shadow<COUNT><<<grid_for((const void *)k_shadow<COUNT>, bound * (A.light_end - A.light_begin)), block, 0, stream>>>(S, F, A);
+            if (timer) timer->end(STAGE_SHADOW, stream);
+        }
+        A.counters = stage_counters(STAGE_SHADE);
+        if (timer) timer->begin(STAGE_SHADE, stream);
+        k_shade<COUNT><<<grid_for((const void *)k_shade<COUNT>, bound), block, 0, stream>>>(S, F, A);
+        if (timer) timer->end(STAGE_SHADE, stream);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace dev
 
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream) {
-    return launch_render_fused(S, F, block, stream);
+                                    cudaStream_t stream, StageTimer *timer) {
+    if (F.settings.render_mode != SLIM_RENDER_BEAUTY)   // a single primary hit: nothing to queue
+        return launch_render_fused(S, F, block, stream, timer);
+    if (F.settings.max_depth == 0) return launch_render_fused(S, F, block, stream, timer);
+    if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer);
+    return dev::run_frame<false>(S, F, B, block, stream, timer);
 }
 
 }  // namespace slim

@@ -88,10 +88,12 @@ PROJECTION = _dt([("inverted_camera_rotation", (f4, 9), 0), ("start", (f4, 3), 3
 SETTINGS = _dt([("max_depth", u1, 0), ("skybox_color_texture_id", i1, 1), ("skybox_radiance_texture_id", i1, 2),
                 ("skybox_irradiance_texture_id", i1, 3), ("render_mode", i4, 4), ("mip_level_colors", (i4, 9), 8)], 44)
 RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4, 8), ("block_size", i4, 12),
-                      ("count_work", i4, 16), ("_reserved", (i4, 3), 20)], 32)
+                      ("count_work", i4, 16), ("profile_stages", i4, 20), ("shadow_queue_mb", i4, 24),
+                      ("_reserved", i4, 28)], 32)
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(
     ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",
      "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels"])], 80)
+STAGE_STATS = _dt([("name", "S24", 0), ("launches", u4, 24), ("total_ms", f4, 28), ("work", WORK_COUNTERS, 32)], 112)
 CAMERA = np.dtype([("orientation", f4, 9), ("position", f4, 3), ("focal_length", f4)])
 
 for _name, _dtype, _size in [("GEOMETRY", GEOMETRY, 72), ("MATERIAL", MATERIAL, 68), ("LIGHT", LIGHT, 32),

@@ -23,6 +23,7 @@ EXPORTS = [
     "slimGetRenderOptions", "slimRenderToDevice", "slimTracePrimary", "slimGetWorkCounters", "slimRefitSceneBVH",
     "slimProjectionReset", "slimBuildSceneBVH", "slimBuildMesh", "slimReadMeshHeader", "slimReadMesh",
     "slimWriteMesh", "slimReadTextureHeader", "slimReadTexture", "slimWriteTexture", "slimBakeTexture",
+    "slimGetStageStats", "slimResetStageStats",
 ]
 
 
@@ -65,6 +66,8 @@ def lib():
     h.slimReadTexture.argtypes = [C.c_char_p, P, P, P]
     h.slimWriteTexture.argtypes = [C.c_char_p, P]
     h.slimBakeTexture.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
+    h.slimGetStageStats.argtypes = [P, C.c_int, P]
+    h.slimResetStageStats.argtypes = []
     for name in EXPORTS:
         if name not in ("slimGetLastError",):
             getattr(h, name).restype = C.c_int
@@ -98,11 +101,28 @@ def projection_reset(orientation9, position3, focal_length, width, height, ssaa=
 
 
 def set_render_options(engine=L.ENGINE_WAVEFRONT, ray_cones=L.CONES_REFERENCE, scene_bvh=L.SCENE_BVH_UPLOADED,
-                       block_size=0, count_work=False):
+                       block_size=0, count_work=False, profile_stages=False, shadow_queue_mb=0):
     o = np.zeros((), L.RENDER_OPTIONS)
     o["engine"], o["ray_cones"], o["scene_bvh"] = engine, ray_cones, scene_bvh
     o["block_size"], o["count_work"] = block_size, int(bool(count_work))
+    o["profile_stages"], o["shadow_queue_mb"] = int(bool(profile_stages)), shadow_queue_mb
     check(lib().slimSetRenderOptions(ptr(o)))
+
+
+def stage_stats():
+    """Per-stage launches, CUDA-event milliseconds and work counters."""
+    out = np.zeros(16, L.STAGE_STATS)
+    count = np.zeros(1, np.int32)
+    check(lib().slimGetStageStats(ptr(out), len(out), ptr(count)))
+    res = []
+    for rec in out[:int(count[0])]:
+        res.append({"name": rec["name"].decode(), "launches": int(rec["launches"]), "total_ms": float(rec["total_ms"]),
+                    "work": {k: int(rec["work"][k]) for k in L.WORK_COUNTERS.names}})
+    return res
+
+
+def reset_stage_stats():
+    check(lib().slimResetStageStats())
 
 
 def work_counters():

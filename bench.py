@@ -234,16 +234,25 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
 
-    # one counted frame: rays per frame and algorithmic bytes per stage
-    native.set_render_options(engine=engine, count_work=True, profile_stages=True)
+    # Counted frames (untimed).  The fused kernel walks every ray in the
+    # reference's order: its counters are the reference algorithm's work for
+    # the frame.  The timed engine's own counters give each stage's work.
     d_pix = torch.empty((n, 4), dtype=torch.float32, device=dev)
     d_dep = torch.empty(n, dtype=torch.float32, device=dev)
+    native.set_render_options(engine=L.ENGINE_MEGAKERNEL, count_work=True)
     native.check(lib.slimRefitSceneBVH(sp))
     r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
     torch.cuda.synchronize()
     work = native.work_counters()
+    native.set_render_options(engine=engine, count_work=True, profile_stages=True)
+    native.reset_stage_stats()
+    native.check(lib.slimRefitSceneBVH(sp))
+    r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
+    torch.cuda.synchronize()
     stage_work = {s["name"]: s["work"] for s in native.stage_stats()}
     rays_per_frame = work["primary_rays"] + work["shadow_rays"] + work["bounce_rays"]
+    engine_work = native.work_counters()
+    assert engine_work["primary_rays"] + engine_work["shadow_rays"] + engine_work["bounce_rays"] == rays_per_frame
 
     # timed device-resident frames
     native.set_render_options(engine=engine, profile_stages=True)

@@ -82,6 +82,7 @@ struct Context {
     DevArray<float4> w_color, w_through, w_rays0, w_rays1, w_hits, w_shadow_rays;
     DevArray<uint32_t> w_counts;
     DevArray<unsigned long long> w_shadow_mask;
+    DevArray<uint4> w_pairs;
     struct EventTimer *timer = nullptr;
 };
 
@@ -127,7 +128,7 @@ struct EventTimer : StageTimer {
         for (int i = 0; i < STAGE_COUNT; i++) { launches[i] = 0; total_ms[i] = 0; }
     }
 };
-const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit"};
+const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit", "shadow_mesh"};
 SlimWorkCounters g_stage_work[STAGE_COUNT];
 
 Context g_ctx;
@@ -525,7 +526,16 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     if (shadow > max_shadow) shadow = max_shadow < samples ? samples : max_shadow;
     if (shadow > 0xFFFFFFFFull) shadow = 0xFFFFFFFFull;
     if ((uint64_t)samples << 6 > 0xFFFFFFFFull) return set_error(SLIM_ERR_LIMIT, "frame too large for the wavefront queues");
-    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= shadow) return SLIM_OK;
+    size_t meshes = c.scene.mesh_count ? c.scene.mesh_count : 1;
+    size_t instances = 0;
+    for (const SlimGeometry &g : c.geometries) instances += g.type == SLIM_GEOMETRY_MESH;
+    size_t pairs = shadow * (instances < 4 ? (instances ? instances : 1) : 4);
+    size_t max_pairs = budget / sizeof(uint4);
+    if (pairs > max_pairs) pairs = max_pairs;
+    if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
+    (void)meshes;
+    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= shadow && c.wavefront.pair_capacity >= pairs)
+        return SLIM_OK;
     uint32_t n = samples;
     int rc = 0;
     if ((rc = c.w_color.reserve(n, "alloc path colour"))) return rc;
@@ -536,6 +546,7 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     if ((rc = c.w_shadow_rays.reserve(2 * shadow, "alloc shadow queue"))) return rc;
     if ((rc = c.w_counts.reserve(8, "alloc queue counters"))) return rc;
     if ((rc = c.w_shadow_mask.reserve(n, "alloc shadow masks"))) return rc;
+    if ((rc = c.w_pairs.reserve(pairs ? pairs : 1, "alloc shadow candidate pairs"))) return rc;
     WavefrontBuffers &B = c.wavefront;
     B.path_color = c.w_color.ptr;
     B.path_throughput = c.w_through.ptr;
@@ -547,6 +558,8 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     B.shadow_mask = c.w_shadow_mask.ptr;
     B.capacity = n;
     B.shadow_capacity = (uint32_t)shadow;
+    B.pairs = c.w_pairs.ptr;
+    B.pair_capacity = (uint32_t)pairs;
     return SLIM_OK;
 }
 

@@ -7,7 +7,9 @@ namespace slim {
 
 // Stages of a frame, for per-stage timing and work counters (16 counter
 // slots per stage in DevFrame::counters).
-enum Stage : int { STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_COUNT };
+enum Stage : int {
+    STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_SHADOW_MESH, STAGE_COUNT
+};
 constexpr int kCountersPerStage = 16;
 
 // Optional CUDA-event timing around each stage launch.
@@ -31,12 +33,14 @@ struct WavefrontBuffers {
     float4 *path_color;              // per sample: accumulated colour (xyz), depth (w)
     float4 *path_throughput;         // per sample: throughput (xyz)
     float4 *rays[2];                 // ping-pong ray queues, 2 float4 per ray
-    uint32_t *queue_count;           // [0..1] ray queue lengths, [2] shadow queue length
+    uint32_t *queue_count;           // [0..1] ray queues, [2] shadow queue, [3] pairs, [4] pair cursor
     float4 *hits;                    // 3 float4 per queue slot
     float4 *shadow_rays;             // 2 float4 per shadow ray
     unsigned long long *shadow_mask; // per queue slot: occluded-light bits
+    uint4 *pairs;                    // shadow ray x mesh instance candidates
     uint32_t capacity;               // samples
     uint32_t shadow_capacity;        // shadow ray slots
+    uint32_t pair_capacity;          // candidate pair slots
 };
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
                                     cudaStream_t stream, StageTimer *timer);

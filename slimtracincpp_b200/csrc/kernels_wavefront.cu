@@ -87,6 +87,10 @@ struct QueueArgs {
     float4 *shadow_rays;
     uint32_t *shadow_count;
     unsigned long long *masks;    // per slot: bit i = light i occluded
+    uint4 *pairs;                 // shadow ray x mesh instance candidates: (ray, geometry, aux distance, 0)
+    uint32_t *pair_count;
+    uint32_t *pair_cursor;
+    uint32_t pair_capacity;
     float4 *path_color;           // per sample: colour, depth
     float4 *path_throughput;      // per sample: throughput
     uint32_t samples;
@@ -188,21 +192,224 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, Queu
 }
 
 // ---- shadow: any-hit tests ------------------------------------------------
+//
+// An any-hit result is the OR, over every (scene leaf, geometry) the segment
+// reaches, of that geometry's test with the leaf's aux distance
+// min(leaf far + EPS, max distance) (scene/scene_tracer.h:111-136): the
+// culling distance never shrinks before the first hit ends the search, so
+// the result does not depend on the order the candidates are tested in.
+// The shadow stage uses that freedom:
+//   shadow_scene  walks the scene BVH per shadow ray, tests implicit
+//                 primitives on the spot and appends one (ray, mesh
+//                 instance, aux distance) pair per reached mesh instance;
+//   shadow_mesh   a persistent kernel in which every lane runs one mesh BVH
+//                 traversal step per loop turn and fetches the next pair as
+//                 soon as its own finishes, so warps stay full although
+//                 traversal lengths differ by orders of magnitude.
+
+SLIM_D bool local_box_test(const DevScene &S, const Geo &g, const Ray &local) {
+    float mn[3], mx[3], n, f;
+    if (g.type == SLIM_GEOMETRY_MESH) {
+        const DevMesh &m = S.meshes[g.mesh];
+        for (int i = 0; i < 3; i++) { mn[i] = m.aabb_min[i]; mx[i] = m.aabb_max[i]; }
+    } else {
+        float e = g.type == SLIM_GEOMETRY_TET ? kTetMax : 1.0f;
+        mx[0] = mx[1] = mx[2] = e;
+        mn[0] = mn[1] = mn[2] = -e;
+        if (g.type == SLIM_GEOMETRY_QUAD) { mn[1] = -kEps; mx[1] = kEps; }
+    }
+    return hit_aabb(local, mn[0], mn[1], mn[2], mx[0], mx[1], mx[2], n, f);
+}
+
+// Candidates of one scene leaf: implicit primitives are tested here, mesh
+// instances become pairs.  Returns true once the ray is known occluded.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow(DevScene S, DevFrame F, QueueArgs A) {
+SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t q, uint32_t first, uint32_t count, float lf,
+                        const Ray &ray, float max_distance, uint32_t *mesh_stack, uint32_t &err, Work &w) {
+    float aux = minr(lf + kEps, max_distance);
+    for (uint32_t i = 0; i < count; i++) {
+        uint32_t gi = __ldg(S.leaf_geometry + first + i);
+        Geo g = load_geo(S, gi);
+        if (!(g.flags & SLIM_GEOMETRY_IS_SHADOWING)) continue;
+        bump<COUNT>(w.geometries);
+        Ray local;
+        localize(local, ray.o, ray.d, g);
+        if (!local_box_test(S, g, local)) continue;
+        bool transparent = (g.flags & SLIM_GEOMETRY_IS_TRANSPARENT) != 0;
+        Hit h;
+        h.distance = aux;
+        switch (g.type) {
+            case SLIM_GEOMETRY_QUAD: if (hit_quad(local, h, transparent)) return true; break;
+            case SLIM_GEOMETRY_BOX: if (hit_box(local, h, transparent)) return true; break;
+            case SLIM_GEOMETRY_SPHERE: if (hit_sphere(local, h, transparent, nullptr)) return true; break;
+            case SLIM_GEOMETRY_TET: if (hit_tet(local, h, transparent)) return true; break;
+            case SLIM_GEOMETRY_MESH: {
+                uint32_t slot = warp_append(A.pair_count, true);
+                if (slot < A.pair_capacity) {
+                    A.pairs[slot] = make_uint4(q, gi, __float_as_uint(aux), 0u);
+                } else if (mesh_trace<COUNT>(S, S.meshes[g.mesh], local, h, true, mesh_stack, err, w)) {
+                    return true;   // pair queue full: trace the instance here
+                }
+            } break;
+            default: break;
+        }
+    }
+    return false;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow_scene(DevScene S, DevFrame F, QueueArgs A) {
     uint32_t n = *A.shadow_count;
     uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
     uint32_t err = 0;
     Work w = {};
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         float4 a = A.shadow_rays[2 * (size_t)q], b = A.shadow_rays[2 * (size_t)q + 1];
+        uint32_t tag = __float_as_uint(a.w);
         Ray ray;
-        ray.o = xyz(a);
-        ray.d = xyz(b);
-        Hit hit;
-        if (scene_trace<COUNT>(S, ray, hit, true, b.w, stack, mesh_stack, err, w) >= 0) {
-            uint32_t tag = __float_as_uint(a.w);
-            atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
+        float3 d = xyz(b);
+        reset(ray, scale_add(d, kTraceOffset, xyz(a)), d);
+        float Ld = b.w;
+        bool occluded = false;
+        float ln, rn, lf, rf;
+        float4 ra, rb;
+        load_node(S.scene_nodes, 0, ra, rb);
+        bump<COUNT>(w.scene_nodes);
+        if (hit_node(ray, ra, rb, ln, lf) && ln < Ld) {
+            if (node_leaf_count(rb)) {
+                occluded = shadow_leaf<COUNT>(S, A, q, 0, S.geometry_count, lf, ray, Ld, mesh_stack, err, w);
+            } else {
+                uint32_t left = node_first(rb), top = 0;
+                for (;;) {
+                    float4 la, lb, xa, xb;
+                    load_node(S.scene_nodes, left, la, lb);
+                    load_node(S.scene_nodes, left + 1, xa, xb);
+                    bump<COUNT>(w.scene_nodes, 2);
+                    bool hl = hit_node(ray, la, lb, ln, lf) && ln < Ld;
+                    bool hr = hit_node(ray, xa, xb, rn, rf) && rn < Ld;
+                    uint32_t lc = node_first(lb), rc = node_first(xb);
+                    bool go_left = hl && !node_leaf_count(lb), go_right = hr && !node_leaf_count(xb);
+                    if (hl && node_leaf_count(lb) &&
+                        shadow_leaf<COUNT>(S, A, q, lc, node_leaf_count(lb), lf, ray, Ld, mesh_stack, err, w)) {
+                        occluded = true;
+                        break;
+                    }
+                    if (hr && node_leaf_count(xb) &&
+                        shadow_leaf<COUNT>(S, A, q, rc, node_leaf_count(xb), rf, ray, Ld, mesh_stack, err, w)) {
+                        occluded = true;
+                        break;
+                    }
+                    if (go_left) {
+                        if (go_right) {
+                            if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; break; }
+                            stack[top++] = rc;
+                        }
+                        left = lc;
+                    } else if (go_right) {
+                        left = rc;
+                    } else {
+                        if (top == 0) break;
+                        left = stack[--top];
+                    }
+                }
+            }
+        }
+        if (occluded) atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
+    }
+    if (err) atomicOr(F.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// One any-hit traversal step of a mesh BVH (MeshTracer::trace with
+// any_hit, scene/mesh_tracer.h:51-114): test the child pair at `left`,
+// triangles of hit leaves, then descend, or pop.  Returns 1 on a hit,
+// -1 when the traversal is over without one, 0 to continue.
+template <bool COUNT>
+SLIM_D int mesh_any_step(const DevScene &S, const float4 *nodes, uint32_t tri_offset, const Ray &r, float aux,
+                         uint32_t &left, uint32_t *stack, uint32_t &top, uint32_t &err, Work &w) {
+    float ln, rn, lf, rf;
+    float4 la, lb, xa, xb;
+    load_node(nodes, left, la, lb);
+    load_node(nodes, left + 1, xa, xb);
+    bump<COUNT>(w.mesh_nodes, 2);
+    bool hl = hit_node(r, la, lb, ln, lf) && ln < aux;
+    bool hr = hit_node(r, xa, xb, rn, rf) && rn < aux;
+    uint32_t lc = node_first(lb), rc = node_first(xb);
+    uint32_t lcount = node_leaf_count(lb), rcount = node_leaf_count(xb);
+    Hit h;
+    h.distance = aux;
+    if (hl && lcount && hit_triangles<COUNT>(S.tri_hot, tri_offset + lc, lcount, lf, r, h, true, w)) return 1;
+    if (hr && rcount && hit_triangles<COUNT>(S.tri_hot, tri_offset + rc, rcount, rf, r, h, true, w)) return 1;
+    bool go_left = hl && !lcount, go_right = hr && !rcount;
+    if (go_left) {
+        if (go_right) {
+            if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; return -1; }
+            stack[top++] = rc;
+        }
+        left = lc;
+    } else if (go_right) {
+        left = rc;
+    } else {
+        if (top == 0) return -1;
+        left = stack[--top];
+    }
+    return 0;
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
+    const uint32_t n = *A.pair_count < A.pair_capacity ? *A.pair_count : A.pair_capacity;
+    uint32_t stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    bool busy = false;
+    uint32_t tag = 0, left = 0, top = 0, tri_offset = 0;
+    const float4 *nodes = nullptr;
+    float aux = 0.0f;
+    Ray r;
+    for (;;) {
+        if (!busy) {
+            // idle lanes of the warp take consecutive pairs with one atomic
+            uint32_t active = __activemask();
+            int leader = __ffs(active) - 1;
+            uint32_t base = 0;
+            if ((int)lane_id() == leader) base = atomicAdd(A.pair_cursor, (uint32_t)__popc(active));
+            base = __shfl_sync(active, base, leader);
+            uint32_t idx = base + (uint32_t)__popc(active & ((1u << lane_id()) - 1u));
+            if (idx >= n) break;
+            uint4 p = A.pairs[idx];
+            float4 a = A.shadow_rays[2 * (size_t)p.x], b = A.shadow_rays[2 * (size_t)p.x + 1];
+            tag = __float_as_uint(a.w);
+            if ((A.masks[tag >> 6] >> (tag & 63u)) & 1ull) continue;   // already known occluded
+            Geo g = load_geo(S, p.y);
+            Ray ray;
+            float3 d = xyz(b);
+            reset(ray, scale_add(d, kTraceOffset, xyz(a)), d);
+            localize(r, ray.o, ray.d, g);
+            aux = __uint_as_float(p.z);
+            const DevMesh &m = S.meshes[g.mesh];
+            nodes = S.mesh_nodes + 2 * (size_t)m.node_offset;
+            tri_offset = m.tri_offset;
+            float ln, lf;
+            float4 ra, rb;
+            load_node(nodes, 0, ra, rb);
+            bump<COUNT>(w.mesh_nodes);
+            if (!(hit_node(r, ra, rb, ln, lf) && ln < aux)) continue;
+            if (node_leaf_count(rb)) {
+                Hit h;
+                h.distance = aux;
+                if (hit_triangles<COUNT>(S.tri_hot, tri_offset, m.tri_count, lf, r, h, true, w))
+                    atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
+                continue;
+            }
+            left = node_first(rb);
+            top = 0;
+            busy = true;
+        }
+        int res = mesh_any_step<COUNT>(S, nodes, tri_offset, r, aux, left, stack, top, err, w);
+        if (res) {
+            if (res > 0) atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
+            busy = false;
         }
     }
     if (err) atomicOr(F.error_flags, err);
@@ -321,6 +528,10 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     A.hits = B.hits;
     A.shadow_rays = B.shadow_rays;
     A.masks = B.shadow_mask;
+    A.pairs = B.pairs;
+    A.pair_count = B.queue_count + 3;
+    A.pair_cursor = B.queue_count + 4;
+    A.pair_capacity = B.pair_capacity;
     A.path_color = B.path_color;
     A.path_throughput = B.path_throughput;
     A.samples = samples;
@@ -355,10 +566,16 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
             if (timer) timer->begin(STAGE_SHADOW_GEN, stream);
             k_shadow_gen<COUNT><<<grid_for((const void *)k_shadow_gen<COUNT>, bound), block, 0, stream>>>(S, F, A);
             if (timer) timer->end(STAGE_SHADOW_GEN, stream);
+            e = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
+            if (e != cudaSuccess) return e;
             A.counters = stage_counters(STAGE_SHADOW);
             if (timer) timer->begin(STAGE_SHADOW, stream);
-            k_shadow<COUNT><<<grid_for((const void *)k_shadow<COUNT>, bound * (A.light_end - A.light_begin)), block, 0, stream>>>(S, F, A);
+            k_shadow_scene<COUNT><<<grid_for((const void *)k_shadow_scene<COUNT>, bound * (A.light_end - A.light_begin)), block, 0, stream>>>(S, F, A);
             if (timer) timer->end(STAGE_SHADOW, stream);
+            A.counters = stage_counters(STAGE_SHADOW_MESH);
+            if (timer) timer->begin(STAGE_SHADOW_MESH, stream);
+            k_shadow_mesh<COUNT><<<grid_for((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), block, 0, stream>>>(S, F, A);
+            if (timer) timer->end(STAGE_SHADOW_MESH, stream);
         }
         A.counters = stage_counters(STAGE_SHADE);
         if (timer) timer->begin(STAGE_SHADE, stream);

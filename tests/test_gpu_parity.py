@@ -131,6 +131,12 @@ def test_work_counters_match_oracle(engine):
     finally:
         native.set_render_options(engine=engine)
     _, _, ref = O.oracle_render(w.scene, w.projection(), w.settings, w.width, w.height, layout=L, count=True)
-    for k in ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",
-              "geometry_tests", "mesh_hit_fetches"]:
+    # The fused kernel walks every ray in the reference's order, so all its
+    # work counts equal the oracle's.  The wavefront engine tests shadow
+    # candidates in another (equally valid) order, so only its ray counts
+    # are fixed.
+    keys = ["primary_rays", "shadow_rays", "bounce_rays"]
+    if engine == L.ENGINE_MEGAKERNEL:
+        keys += ["scene_node_tests", "mesh_node_tests", "triangle_tests", "geometry_tests", "mesh_hit_fetches"]
+    for k in keys:
         assert got[k] == ref[k], (k, got[k], ref[k])

@@ -268,6 +268,23 @@ int slimRenderToDevice(const SlimCanvasData *canvas, const SlimCameraRayProjecti
                        const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths,
                        void *stream);
 
+/* No counterpart in the reference.  Same frame as slimRenderToDevice with
+ * the wavefront engine, but allocates nothing: for callers that cannot
+ * enter the CUDA allocator from their per-frame hook -- e.g. while another
+ * thread captures a CUDA graph in global capture mode, which makes
+ * cudaMalloc/cudaFree fail process-wide, or inside a host engine that
+ * reserves all device memory up front.  The queues live in one file-scope
+ * __device__ array of 64 MiB that every GPU loading the library holds until
+ * exit; frames needing more (about 250 bytes per sample, e.g. 640x360 with
+ * several lights fits, 1080p does not) fail with SLIM_ERR_LIMIT.  The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  Every call shares the one array: calls whose work overlaps on
+ * the GPU (different streams, or threads without ordering) race and corrupt
+ * each other's frames.  Debug render modes and max_depth 0 use no scratch. */
+int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                              const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths, void *stream);
+
 /* Closest hit of every primary ray (renderer/ray_tracer.h:36-45 ->
  * scene/scene_tracer.h:26-98) into device buffers of width*height entries:
  * geometry index (-1 = miss), mesh triangle id in leaf order (0 for

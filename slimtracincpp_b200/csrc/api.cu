@@ -823,3 +823,115 @@ int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Frame rendering that allocates nothing.
+//
+// The ordinary entry points size the wavefront queues with cudaMalloc on
+// the first frame of a size (hundreds of MiB at 1080p).  Some callers of a
+// per-frame render hook cannot enter the CUDA allocator: an application
+// whose other thread is capturing a CUDA graph in global capture mode (the
+// runtime then refuses cudaMalloc/cudaFree from every thread), or a host
+// engine that reserves the device memory up front and forbids allocation
+// inside its frame loop.  slimRenderToDeviceNoAlloc gives them the
+// wavefront render with its queues carved out of one file-scope device
+// array of fixed size instead.
+namespace slim {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;   // held by every GPU that loads the library
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+unsigned char *g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of this device's copy of the array, looked up once per
+// device (host code may only use the symbol through this address).
+int noalloc_scratch(unsigned char **out) {
+    int device = 0;
+    SLIM_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+    if (device < 0 || device >= kNoAllocMaxDevices) return set_error(SLIM_ERR_LIMIT, "device index beyond 64");
+    if (!g_noalloc_base[device]) {
+        void *p = nullptr;
+        SLIM_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_base[device] = (unsigned char *)p;
+    }
+    *out = g_noalloc_base[device];
+    return SLIM_OK;
+}
+
+// Carves the wavefront queues for `samples` out of the scratch: 152 bytes
+// per sample of path state, ray queues, hit records and shadow masks, then
+// the shadow-ray queue for as many lights per batch as fit (at least one)
+// and the shadow candidate pairs in the rest.
+int noalloc_layout(unsigned char *base, uint32_t samples, uint32_t lights, WavefrontBuffers &B) {
+    auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    size_t n = samples, off = 0;
+    auto take = [&](size_t bytes) { unsigned char *p = base + off; off = up(off + bytes); return p; };
+    B.path_color = (float4 *)take(16 * n);
+    B.path_throughput = (float4 *)take(16 * n);
+    B.rays[0] = (float4 *)take(32 * n);
+    B.rays[1] = (float4 *)take(32 * n);
+    B.hits = (float4 *)take(48 * n);
+    B.shadow_mask = (unsigned long long *)take(8 * n);
+    B.queue_count = (uint32_t *)take(8 * sizeof(uint32_t));
+    if (off > kNoAllocScratchBytes) return set_error(SLIM_ERR_LIMIT, "frame larger than the no-alloc scratch (64 MiB)");
+    size_t left = kNoAllocScratchBytes - off;
+    size_t per_light = n * (32 + 16);           // one shadow ray + at least one candidate pair per sample and light
+    size_t batch = per_light ? left / per_light : 0;
+    if (batch < 1) return set_error(SLIM_ERR_LIMIT, "frame larger than the no-alloc scratch (64 MiB)");
+    if (batch > lights) batch = lights ? lights : 1;
+    size_t shadow = n * batch;
+    B.shadow_rays = (float4 *)take(32 * shadow);
+    size_t pairs = (kNoAllocScratchBytes - off) / 16;
+    B.pairs = (uint4 *)(base + off);
+    if (shadow > 0xFFFFFFFFull) shadow = 0xFFFFFFFFull;
+    if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
+    B.capacity = samples;
+    B.shadow_capacity = (uint32_t)shadow;
+    B.pair_capacity = (uint32_t)pairs;
+    return SLIM_OK;
+}
+
+}  // namespace
+}  // namespace slim
+
+extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                                         const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths,
+                                         void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!canvas || !projection || !settings || !d_pixels || !d_depths)
+        return set_error(SLIM_ERR_ARGUMENT, "slimRenderToDeviceNoAlloc: null argument");
+    const SlimDimensions &dim = canvas->dimensions;
+    if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
+    if (canvas->antialias < SLIM_AA_NONE || canvas->antialias > SLIM_AA_SSAA) return set_error(SLIM_ERR_ARGUMENT, "bad antialias mode");
+    int rc = check_settings(c, settings);
+    if (rc) return rc;
+    uint32_t s = canvas->antialias == SLIM_AA_SSAA ? 2 : 1;
+    DevFrame F;
+    memset(&F, 0, sizeof(F));
+    F.projection = *projection;
+    F.settings = *settings;
+    F.width = (uint32_t)dim.width * s;
+    F.height = (uint32_t)dim.height * s;
+    F.stride = dim.stride ? dim.stride : dim.width;
+    if (F.stride < dim.width) return set_error(SLIM_ERR_ARGUMENT, "canvas stride below width");
+    F.antialias = canvas->antialias;
+    F.cones_per_pixel = c.options.ray_cones == SLIM_CONES_PER_PIXEL;
+    F.pixels = (float4 *)d_pixels;
+    F.depths = (float *)d_depths;
+    F.error_flags = c.d_error.ptr;
+    F.counters = nullptr;
+    unsigned char *scratch = nullptr;
+    if ((rc = noalloc_scratch(&scratch))) return rc;
+    WavefrontBuffers B;
+    memset(&B, 0, sizeof(B));
+    if ((rc = noalloc_layout(scratch, F.width * F.height, c.scene.light_count, B))) return rc;
+    // The queue counters at the head of the scratch are zeroed by the
+    // launcher (cudaMemsetAsync) before the first stage reads them; every
+    // other region is written before it is read within the frame.
+    cudaError_t e = launch_render_wavefront(c.scene, F, B, c.options.block_size, (cudaStream_t)stream, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "no-alloc render launch");
+    return SLIM_OK;
+}

@@ -23,7 +23,7 @@ EXPORTS = [
     "slimGetRenderOptions", "slimRenderToDevice", "slimTracePrimary", "slimGetWorkCounters", "slimRefitSceneBVH",
     "slimProjectionReset", "slimBuildSceneBVH", "slimBuildMesh", "slimReadMeshHeader", "slimReadMesh",
     "slimWriteMesh", "slimReadTextureHeader", "slimReadTexture", "slimWriteTexture", "slimBakeTexture",
-    "slimGetStageStats", "slimResetStageStats",
+    "slimGetStageStats", "slimResetStageStats", "slimRenderToDeviceNoAlloc",
 ]
 
 
@@ -56,6 +56,7 @@ def lib():
         getattr(h, name).restype = C.c_int
     h.slimRenderOnGPU.argtypes = [P, P, P]
     h.slimRenderToDevice.argtypes = [P, P, P, P, P, P]
+    h.slimRenderToDeviceNoAlloc.argtypes = [P, P, P, P, P, P]
     h.slimTracePrimary.argtypes = [P, C.c_int, C.c_int, P, P, P, P, P]
     h.slimProjectionReset.argtypes = [P, P, C.c_float, C.c_int, C.c_int, C.c_int, P]
     h.slimBuildMesh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, P, P, P]

@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--config", default="config2", choices=["config1", "config2", "config3"],
+                   help="workload (default: config2, the metric's 1080p mesh PBR scene)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     return p.parse_args()
@@ -180,7 +182,7 @@ def run_reference(args):
         return 0
     from slimtracincpp_b200 import scenes
     from oracle import bindings as O
-    w = scenes.config2(args.seed)
+    w = scenes.CONFIGS[args.config](args.seed)
     if not O.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libslimref.so was not built"}))
         return 0
@@ -198,9 +200,10 @@ def run_reference(args):
     frame_rays = None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(1, args.steps), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 scene)",
-            "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 2,
-                       "instances": 8, "triangles": 81920 + 130050, "parallelism": "host threads"},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.config} scene)",
+            "config": {"workload": w.name, "width": w.width, "height": w.height,
+                       "max_depth": int(w.settings["max_depth"]), "geometries": len(w.scene.geometries),
+                       "triangles": sum(m.triangle_count for m in w.scene.meshes), "parallelism": "host threads"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": vals[0]["kind"],
                              "sample": vals[0]["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -226,9 +229,11 @@ def main():
     from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport, make_canvas
 
     engine = L.ENGINE_WAVEFRONT if args.engine == "wavefront" else L.ENGINE_MEGAKERNEL
-    w = scenes.config2(args.seed)
+    w = scenes.CONFIGS[args.config](args.seed)
     lib = native.lib()
-    r = RayTracingRenderer(w.scene, max_depth=int(w.settings["max_depth"]))
+    st = w.settings
+    r = RayTracingRenderer(w.scene, int(st["max_depth"]), int(st["skybox_color_texture_id"]),
+                           int(st["skybox_radiance_texture_id"]), int(st["skybox_irradiance_texture_id"]))
     vp = Viewport(w.camera, w.width, w.height)
     n = w.samples
     stream = torch.cuda.current_stream(dev)
@@ -339,9 +344,12 @@ def main():
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-2 scene)",
-            "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 2, "instances": 8,
-                       "triangles": 81920 + 130050, "engine": args.engine, "parallelism": f"replicas x{world}",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.config} scene)",
+            "config": {"workload": w.name, "width": w.width, "height": w.height,
+                       "max_depth": int(w.settings["max_depth"]), "geometries": len(w.scene.geometries),
+                       "triangles": sum(m.triangle_count for m in w.scene.meshes),
+                       "textures": len(w.scene.textures), "lights": len(w.scene.lights),
+                       "engine": args.engine, "parallelism": f"replicas x{world}",
                        "l2": "flushed between steps (512 MiB write)", "rays_per_frame": rays_per_frame,
                        "primary_rays": work["primary_rays"], "shadow_rays": work["shadow_rays"],
                        "bounce_rays": work["bounce_rays"]},

@@ -82,7 +82,7 @@ struct Context {
     DevArray<float4> w_color, w_through, w_rays0, w_rays1, w_hits, w_shadow_rays;
     DevArray<uint32_t> w_counts;
     DevArray<unsigned long long> w_shadow_mask;
-    DevArray<uint4> w_pairs;
+    DevArray<float4> w_pairs;
     struct EventTimer *timer = nullptr;
 };
 
@@ -345,6 +345,7 @@ int upload_meshes(Context &c, const SlimSceneData *s) {
         total_tris += m.triangle_count;
         if (total_nodes > 0xFFFFFFFFull / 2 || total_tris > 0xFFFFFFFFull / 4) return set_error(SLIM_ERR_LIMIT, "meshes too large");
     }
+
     int rc = c.d_meshes.reserve(metas.size(), "alloc meshes");
     if (rc) return rc;
     SLIM_CUDA(cudaMemcpy(c.d_meshes.ptr, metas.data(), metas.size() * sizeof(DevMesh), cudaMemcpyHostToDevice), "upload meshes");
@@ -530,7 +531,7 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     size_t instances = 0;
     for (const SlimGeometry &g : c.geometries) instances += g.type == SLIM_GEOMETRY_MESH;
     size_t pairs = shadow * (instances < 4 ? (instances ? instances : 1) : 4);
-    size_t max_pairs = budget / sizeof(uint4);
+    size_t max_pairs = budget / (3 * sizeof(float4));
     if (pairs > max_pairs) pairs = max_pairs;
     if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
     (void)meshes;
@@ -546,7 +547,7 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     if ((rc = c.w_shadow_rays.reserve(2 * shadow, "alloc shadow queue"))) return rc;
     if ((rc = c.w_counts.reserve(8, "alloc queue counters"))) return rc;
     if ((rc = c.w_shadow_mask.reserve(n, "alloc shadow masks"))) return rc;
-    if ((rc = c.w_pairs.reserve(pairs ? pairs : 1, "alloc shadow candidate pairs"))) return rc;
+    if ((rc = c.w_pairs.reserve(3 * (pairs ? pairs : 1), "alloc shadow candidate pairs"))) return rc;
     WavefrontBuffers &B = c.wavefront;
     B.path_color = c.w_color.ptr;
     B.path_throughput = c.w_through.ptr;
@@ -876,14 +877,14 @@ int noalloc_layout(unsigned char *base, uint32_t samples, uint32_t lights, Wavef
     B.queue_count = (uint32_t *)take(8 * sizeof(uint32_t));
     if (off > kNoAllocScratchBytes) return set_error(SLIM_ERR_LIMIT, "frame larger than the no-alloc scratch (64 MiB)");
     size_t left = kNoAllocScratchBytes - off;
-    size_t per_light = n * (32 + 16);           // one shadow ray + at least one candidate pair per sample and light
+    size_t per_light = n * (32 + 48);           // one shadow ray + at least one candidate pair per sample and light
     size_t batch = per_light ? left / per_light : 0;
     if (batch < 1) return set_error(SLIM_ERR_LIMIT, "frame larger than the no-alloc scratch (64 MiB)");
     if (batch > lights) batch = lights ? lights : 1;
     size_t shadow = n * batch;
     B.shadow_rays = (float4 *)take(32 * shadow);
-    size_t pairs = (kNoAllocScratchBytes - off) / 16;
-    B.pairs = (uint4 *)(base + off);
+    size_t pairs = (kNoAllocScratchBytes - off) / 48;
+    B.pairs = (float4 *)(base + off);
     if (shadow > 0xFFFFFFFFull) shadow = 0xFFFFFFFFull;
     if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
     B.capacity = samples;

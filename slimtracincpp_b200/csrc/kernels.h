@@ -37,7 +37,7 @@ struct WavefrontBuffers {
     float4 *hits;                    // 3 float4 per queue slot
     float4 *shadow_rays;             // 2 float4 per shadow ray
     unsigned long long *shadow_mask; // per queue slot: occluded-light bits
-    uint4 *pairs;                    // shadow ray x mesh instance candidates
+    float4 *pairs;                   // shadow ray x mesh instance candidates, 3 float4 each
     uint32_t capacity;               // samples
     uint32_t shadow_capacity;        // shadow ray slots
     uint32_t pair_capacity;          // candidate pair slots

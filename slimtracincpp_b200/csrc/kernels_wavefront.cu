@@ -87,7 +87,8 @@ struct QueueArgs {
     float4 *shadow_rays;
     uint32_t *shadow_count;
     unsigned long long *masks;    // per slot: bit i = light i occluded
-    uint4 *pairs;                 // shadow ray x mesh instance candidates: (ray, geometry, aux distance, 0)
+    float4 *pairs;                // shadow ray x mesh instance candidates, 3 float4 each:
+                                  // (local origin, aux distance) (local direction, tag) (nodes, triangles, first child)
     uint32_t *pair_count;
     uint32_t *pair_cursor;
     uint32_t pair_capacity;
@@ -222,9 +223,11 @@ SLIM_D bool local_box_test(const DevScene &S, const Geo &g, const Ray &local) {
 }
 
 // Candidates of one scene leaf: implicit primitives are tested here, mesh
-// instances become pairs.  Returns true once the ray is known occluded.
+// instances whose BVH root the local ray reaches become pairs carrying the
+// local ray, so the mesh pass starts at the root's children.  Returns true
+// once the ray is known occluded.
 template <bool COUNT>
-SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t q, uint32_t first, uint32_t count, float lf,
+SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t tag, uint32_t first, uint32_t count, float lf,
                         const Ray &ray, float max_distance, uint32_t *mesh_stack, uint32_t &err, Work &w) {
     float aux = minr(lf + kEps, max_distance);
     for (uint32_t i = 0; i < count; i++) {
@@ -244,10 +247,25 @@ SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t q, uint3
             case SLIM_GEOMETRY_SPHERE: if (hit_sphere(local, h, transparent, nullptr)) return true; break;
             case SLIM_GEOMETRY_TET: if (hit_tet(local, h, transparent)) return true; break;
             case SLIM_GEOMETRY_MESH: {
+                const DevMesh &m = S.meshes[g.mesh];
+                const float4 *nodes = S.mesh_nodes + 2 * (size_t)m.node_offset;
+                float ln, lf2;
+                float4 ra, rb;
+                load_node(nodes, 0, ra, rb);
+                bump<COUNT>(w.mesh_nodes);
+                if (!(hit_node(local, ra, rb, ln, lf2) && ln < aux)) break;
+                if (node_leaf_count(rb)) {
+                    if (hit_triangles<COUNT>(S.tri_hot, m.tri_offset, m.tri_count, lf2, local, h, true, w)) return true;
+                    break;
+                }
                 uint32_t slot = warp_append(A.pair_count, true);
                 if (slot < A.pair_capacity) {
-                    A.pairs[slot] = make_uint4(q, gi, __float_as_uint(aux), 0u);
-                } else if (mesh_trace<COUNT>(S, S.meshes[g.mesh], local, h, true, mesh_stack, err, w)) {
+                    float4 *p = A.pairs + 3 * (size_t)slot;
+                    p[0] = make_float4(local.o.x, local.o.y, local.o.z, aux);
+                    p[1] = make_float4(local.d.x, local.d.y, local.d.z, __uint_as_float(tag));
+                    p[2] = make_float4(__uint_as_float(m.node_offset), __uint_as_float(m.tri_offset),
+                                       __uint_as_float(node_first(rb)), 0.0f);
+                } else if (mesh_trace<COUNT>(S, m, local, h, true, mesh_stack, err, w)) {
                     return true;   // pair queue full: trace the instance here
                 }
             } break;
@@ -277,7 +295,7 @@ __global__ void __launch_bounds__(256) k_shadow_scene(DevScene S, DevFrame F, Qu
         bump<COUNT>(w.scene_nodes);
         if (hit_node(ray, ra, rb, ln, lf) && ln < Ld) {
             if (node_leaf_count(rb)) {
-                occluded = shadow_leaf<COUNT>(S, A, q, 0, S.geometry_count, lf, ray, Ld, mesh_stack, err, w);
+                occluded = shadow_leaf<COUNT>(S, A, tag, 0, S.geometry_count, lf, ray, Ld, mesh_stack, err, w);
             } else {
                 uint32_t left = node_first(rb), top = 0;
                 for (;;) {
@@ -290,12 +308,12 @@ __global__ void __launch_bounds__(256) k_shadow_scene(DevScene S, DevFrame F, Qu
                     uint32_t lc = node_first(lb), rc = node_first(xb);
                     bool go_left = hl && !node_leaf_count(lb), go_right = hr && !node_leaf_count(xb);
                     if (hl && node_leaf_count(lb) &&
-                        shadow_leaf<COUNT>(S, A, q, lc, node_leaf_count(lb), lf, ray, Ld, mesh_stack, err, w)) {
+                        shadow_leaf<COUNT>(S, A, tag, lc, node_leaf_count(lb), lf, ray, Ld, mesh_stack, err, w)) {
                         occluded = true;
                         break;
                     }
                     if (hr && node_leaf_count(xb) &&
-                        shadow_leaf<COUNT>(S, A, q, rc, node_leaf_count(xb), rf, ray, Ld, mesh_stack, err, w)) {
+                        shadow_leaf<COUNT>(S, A, tag, rc, node_leaf_count(xb), rf, ray, Ld, mesh_stack, err, w)) {
                         occluded = true;
                         break;
                     }
@@ -377,32 +395,15 @@ __global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, Que
             base = __shfl_sync(active, base, leader);
             uint32_t idx = base + (uint32_t)__popc(active & ((1u << lane_id()) - 1u));
             if (idx >= n) break;
-            uint4 p = A.pairs[idx];
-            float4 a = A.shadow_rays[2 * (size_t)p.x], b = A.shadow_rays[2 * (size_t)p.x + 1];
-            tag = __float_as_uint(a.w);
+            const float4 *p = A.pairs + 3 * (size_t)idx;
+            float4 p0 = p[0], p1 = p[1], p2 = p[2];
+            tag = __float_as_uint(p1.w);
             if ((A.masks[tag >> 6] >> (tag & 63u)) & 1ull) continue;   // already known occluded
-            Geo g = load_geo(S, p.y);
-            Ray ray;
-            float3 d = xyz(b);
-            reset(ray, scale_add(d, kTraceOffset, xyz(a)), d);
-            localize(r, ray.o, ray.d, g);
-            aux = __uint_as_float(p.z);
-            const DevMesh &m = S.meshes[g.mesh];
-            nodes = S.mesh_nodes + 2 * (size_t)m.node_offset;
-            tri_offset = m.tri_offset;
-            float ln, lf;
-            float4 ra, rb;
-            load_node(nodes, 0, ra, rb);
-            bump<COUNT>(w.mesh_nodes);
-            if (!(hit_node(r, ra, rb, ln, lf) && ln < aux)) continue;
-            if (node_leaf_count(rb)) {
-                Hit h;
-                h.distance = aux;
-                if (hit_triangles<COUNT>(S.tri_hot, tri_offset, m.tri_count, lf, r, h, true, w))
-                    atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
-                continue;
-            }
-            left = node_first(rb);
+            reset(r, xyz(p0), xyz(p1));
+            aux = p0.w;
+            nodes = S.mesh_nodes + 2 * (size_t)__float_as_uint(p2.x);
+            tri_offset = __float_as_uint(p2.y);
+            left = __float_as_uint(p2.z);
             top = 0;
             busy = true;
         }

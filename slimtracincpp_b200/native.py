@@ -6,13 +6,15 @@ Loading fails loudly when the in-tree build is missing.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 from . import layout as L
 
-LIB_PATH = Path(__file__).resolve().parent / "_native" / "libslimtracer_b200.so"
+# SLIMTRACER_LIB points at another build of the same library (packaging).
+LIB_PATH = Path(os.environ.get("SLIMTRACER_LIB", Path(__file__).resolve().parent / "_native" / "libslimtracer_b200.so"))
 
 SLIM_OK = 0
 ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "LIMIT", 5: "IO", 6: "STACK"}

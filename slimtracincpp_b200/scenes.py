@@ -20,7 +20,7 @@ from pathlib import Path
 import numpy as np
 
 from . import layout as L
-from .scene import Camera, MeshAsset, Scene, geometry, light, quat_y
+from .scene import Camera, MeshAsset, Scene, TextureAsset, geometry, light, quat_y
 
 ROOT = Path(__file__).resolve().parent.parent
 ASSET_CACHE = Path(os.environ.get("SLIM_ASSET_CACHE", ROOT / "_build" / "assets"))
@@ -279,4 +279,162 @@ def feature_scene(seed=0, width=96, height=54, max_depth=4):
                     L.default_settings(max_depth=max_depth))
 
 
-CONFIGS = {"config1": config1, "config2": config2}
+# ---- textures and sky -------------------------------------------------------
+def albedo_texture(rng, size):
+    """Value-noise RGBA8 albedo (sRGB bytes, B,G,R,A as a BMP stores them),
+    baked with a full mip chain and wrap addressing."""
+    base = rng.uniform(0.15, 0.95, 3)
+    n = value_noise_2d(rng, size, max(2, size // 64))
+    tint = rng.uniform(0.5, 1.0, 3)
+    rgb = np.clip(base[None, None, :] * (0.55 + 0.9 * (n[..., None] - 0.5)) * tint[None, None, :], 0, 1)
+    bgra = np.empty((size, size, 4), np.uint8)
+    bgra[..., 0] = (rgb[..., 2] * 255).astype(np.uint8)
+    bgra[..., 1] = (rgb[..., 1] * 255).astype(np.uint8)
+    bgra[..., 2] = (rgb[..., 0] * 255).astype(np.uint8)
+    bgra[..., 3] = 255
+    return TextureAsset.bake(bgra, L.IMAGE_MIPMAP | L.IMAGE_WRAP)
+
+
+def normal_texture(rng, size, strength=2.0):
+    """Tangent-space normal map of a value-noise height field: X and Y stored
+    in R and G, Z derived by the baker (bmp2texture's -n)."""
+    hgt = value_noise_2d(rng, size, max(2, size // 32)) * strength
+    gy, gx = np.gradient(hgt * size / 16.0)
+    x, y = -gx, -gy
+    inv = 1.0 / np.sqrt(x * x + y * y + 1.0)
+    bgr = np.zeros((size, size, 3), np.uint8)
+    bgr[..., 2] = np.clip((x * inv * 0.5 + 0.5) * 255, 0, 255).astype(np.uint8)
+    bgr[..., 1] = np.clip((y * inv * 0.5 + 0.5) * 255, 0, 255).astype(np.uint8)
+    bgr[..., 0] = 255
+    return TextureAsset.bake(bgr, L.IMAGE_MIPMAP | L.IMAGE_WRAP | L.IMAGE_NORMAL | L.IMAGE_LINEAR)
+
+
+def cube_directions(h):
+    """Unit directions of the texel centres of a 6h x h cube strip laid out
+    as the reference samples it (core/texture.h:72-116): four side faces
+    (left, front, right, back) across the first 4h columns, then the top and
+    bottom faces."""
+    ys = (np.arange(h) + 0.5) / h
+    dirs = np.zeros((h, 6 * h, 3))
+    u4 = (np.arange(4 * h) + 0.5) / (4 * h)
+    U, V = np.meshgrid(u4, ys)
+    face = np.minimum((U * 4).astype(int), 3)
+    d = np.zeros((h, 4 * h, 3))
+    left, front, right, back = face == 0, face == 1, face == 2, face == 3
+    d[left] = np.stack([-np.ones(left.sum()), -(2 * V[left] - 1), -(1 - 8 * U[left])], -1)
+    d[front] = np.stack([8 * U[front] - 3, 1 - 2 * V[front], np.ones(front.sum())], -1)
+    d[right] = np.stack([np.ones(right.sum()), 1 - 2 * V[right], 5 - 8 * U[right]], -1)
+    d[back] = np.stack([7 - 8 * U[back], 1 - 2 * V[back], -np.ones(back.sum())], -1)
+    dirs[:, :4 * h] = d
+    u1 = (np.arange(h) + 0.5) / h
+    U1, V1 = np.meshgrid(u1, ys)
+    dirs[:, 4 * h:5 * h] = np.stack([2 * U1 - 1, np.ones_like(U1), 2 * V1 - 1], -1)
+    dirs[:, 5 * h:] = np.stack([2 * U1 - 1, -np.ones_like(U1), 1 - 2 * V1], -1)
+    return dirs / np.linalg.norm(dirs, axis=-1, keepdims=True)
+
+
+def sky_radiance(dirs, rng):
+    """Procedural sky: zenith/horizon gradient, dark ground, three Gaussian
+    sun lobes; linear RGB in [0, 1]."""
+    y = dirs[..., 1:2]
+    zenith, horizon, ground = np.array([0.18, 0.32, 0.62]), np.array([0.75, 0.78, 0.82]), np.array([0.16, 0.14, 0.12])
+    t = np.clip(y, 0, 1) ** 0.45
+    col = np.where(y >= 0, horizon * (1 - t) + zenith * t, ground + (horizon - ground) * np.exp(8 * y))
+    for _ in range(3):
+        elev = rng.uniform(0.15, 1.0)
+        az = rng.uniform(0, 2 * np.pi)
+        sd = np.array([np.cos(az) * np.sqrt(1 - elev ** 2), elev, np.sin(az) * np.sqrt(1 - elev ** 2)])
+        cosang = np.clip(dirs @ sd, -1, 1)
+        sharp = rng.uniform(200, 900)
+        col = col + rng.uniform(0.5, 0.9) * np.exp(-(1 - cosang)[..., None] * sharp) * rng.uniform(0.8, 1.0, 3)
+    return np.clip(col, 0, 1)
+
+
+def to_bgr8(rgb):
+    out = np.empty(rgb.shape[:2] + (3,), np.uint8)
+    out[..., 0] = (rgb[..., 2] * 255).astype(np.uint8)
+    out[..., 1] = (rgb[..., 1] * 255).astype(np.uint8)
+    out[..., 2] = (rgb[..., 0] * 255).astype(np.uint8)
+    return out
+
+
+def sky_cubes(rng, size=512, irradiance_size=32):
+    """Radiance cube (size) and its cosine-convolved irradiance cube
+    (irradiance_size), both baked as linear 8-bit cube strips (-c -l)."""
+    dirs = cube_directions(size)
+    radiance = sky_radiance(dirs, rng)
+    # irradiance: cosine-weighted average over a coarse copy of the sky
+    coarse = max(8, min(size, 32))
+    cd = cube_directions(coarse).reshape(-1, 3)
+    cr = sky_radiance(cube_directions(coarse), np.random.default_rng(rng.integers(1 << 31)))
+    step = size // coarse
+    cr = radiance[step // 2::step, step // 2::step][:coarse, :6 * coarse].reshape(-1, 3)
+    idirs = cube_directions(irradiance_size).reshape(-1, 3)
+    w = np.clip(idirs @ cd.T, 0, None)
+    irr = (w @ cr) / np.maximum(w.sum(1, keepdims=True), 1e-9)
+    irr = irr.reshape(irradiance_size, 6 * irradiance_size, 3)
+    flags = L.IMAGE_CUBEMAP | L.IMAGE_LINEAR
+    return TextureAsset.bake(to_bgr8(radiance), flags), TextureAsset.bake(to_bgr8(irr), flags)
+
+
+def config3(seed=0, width=1920, height=1080, tex_size=1024, cube_size=512, irradiance_size=32, max_depth=8):
+    """config 1's objects + 4 glass spheres + 2 mirror quads, albedo and
+    normal textures, sky cube IBL."""
+    rng = np.random.default_rng(seed)
+    trng = np.random.default_rng(seed + 1000)
+    textures = [albedo_texture(trng, tex_size) for _ in range(4)] + [normal_texture(trng, tex_size) for _ in range(2)]
+    sky, irr = sky_cubes(trng, cube_size, irradiance_size)
+    textures += [sky, irr]
+    SKY, IRR = 6, 7
+    floor = L.default_material(albedo=0.9, roughness=0.7, brdf=L.BRDF_LAMBERT,
+                               flags=L.MATERIAL_HAS_ALBEDO_MAP | L.MATERIAL_HAS_NORMAL_MAP, texture_ids=(0, 4),
+                               uv_repeat=(4.0, 4.0), normal_magnitude=0.8)
+    materials = [floor]
+    geos = [geometry(L.GEOMETRY_QUAD, 0, (0, 0, 0), (10, 1, 10))]
+    geos += _implicit_objects(rng, materials)
+    # texture the implicit objects (the tetrahedron stays untextured)
+    for k, mid in enumerate(range(1, 6)):
+        m = materials[mid]
+        m["flags"] |= L.MATERIAL_HAS_ALBEDO_MAP | (L.MATERIAL_HAS_NORMAL_MAP if k % 2 == 0 else 0)
+        m["texture_count"] = 2
+        m["texture_ids"] = (1 + k % 3, 4 + k % 2)
+        m["albedo"] = np.float32(1.0)
+    glass = L.default_material(albedo=0.05, roughness=0.25, flags=L.MATERIAL_IS_REFRACTIVE, ior=1.5, reflectivity=0.04)
+    mirror = L.default_material(albedo=0.0, roughness=0.02, flags=L.MATERIAL_IS_REFLECTIVE,
+                                reflectivity=(0.91, 0.92, 0.92))
+    materials += [glass, mirror]
+    GLASS, MIRROR = len(materials) - 2, len(materials) - 1
+    for _ in range(4):
+        r = np.float32(rng.uniform(0.5, 1.2))
+        x, z = rng.uniform(-5, 5, 2)
+        geos.append(geometry(L.GEOMETRY_SPHERE, GLASS, (x, r, z), (r, r, r), flags=L.GEOMETRY_IS_VISIBLE))
+    for sx in (-1, 1):
+        ang = rng.uniform(-0.6, 0.6) + (0.35 if sx > 0 else -0.35)
+        a, w_ = quat_y(ang)
+        # stand the quad up: rotate +y normal to face -z, then turn about y
+        qx = np.array([np.sin(-np.pi / 4), 0, 0, np.cos(-np.pi / 4)])
+        qy = np.array([a[0], a[1], a[2], w_], np.float64)
+        q = _qmul(qy, qx)
+        geos.append(geometry(L.GEOMETRY_QUAD, MIRROR, (sx * 4.5, 2.5, 6.5), (2.5, 1, 2.5), q[:3], q[3]))
+    lights = [light(rng.uniform(0.5, 1.0, 3), (rng.uniform(-5, 5), rng.uniform(3, 6), rng.uniform(-5, 5)),
+                    rng.uniform(5, 20)) for _ in range(2)]
+    scene = Scene(np.array(geos), np.array(materials), np.array(lights), textures=textures)
+    cam = Camera.look_at((0.0, 5.0, -13.0), (0.0, 1.0, 1.0), 60.0)
+    return Workload(f"config3_glass_mirror_textures_ibl_{width}x{height}_d{max_depth}", scene, cam, width, height,
+                    L.default_settings(max_depth=max_depth, skybox_color=SKY, skybox_radiance=SKY,
+                                       skybox_irradiance=IRR))
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return np.array([aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+                     aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz], np.float32)
+
+
+def small_textured_scene(seed=0, width=160, height=90, max_depth=8):
+    """config 3's shape at oracle-friendly size (64^2 textures, 32^2 sky)."""
+    return config3(seed, width, height, tex_size=64, cube_size=32, irradiance_size=8, max_depth=max_depth)
+
+
+CONFIGS = {"config1": config1, "config2": config2, "config3": config3}

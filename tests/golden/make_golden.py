@@ -40,6 +40,7 @@ RENDER_CASES = {
     "render_mesh_normals": lambda: (scenes.small_mesh_scene(6, 64, 36), L.AA_NONE, L.RENDER_NORMALS),
     "render_features": lambda: (scenes.feature_scene(7, 96, 54), L.AA_NONE, None),
     "render_features_depth": lambda: (scenes.feature_scene(8, 64, 36), L.AA_NONE, L.RENDER_DEPTH),
+    "render_textured_ibl": lambda: (scenes.small_textured_scene(9, 64, 36), L.AA_NONE, None),
 }
 
 

@@ -59,6 +59,13 @@ def assert_depths_close(gpu, ref):
     np.testing.assert_allclose(gpu[finite], ref[finite], rtol=1e-5, atol=0)
 
 
+def renderer_for(w, **kw):
+    """A renderer with the workload's settings (depth and skybox ids)."""
+    st = w.settings
+    return RayTracingRenderer(w.scene, int(st["max_depth"]), int(st["skybox_color_texture_id"]),
+                              int(st["skybox_radiance_texture_id"]), int(st["skybox_irradiance_texture_id"]), **kw)
+
+
 def workloads():
     return {
         "config1": lambda: scenes.config1(0, 320, 180),
@@ -66,6 +73,7 @@ def workloads():
         "mesh_small": lambda: scenes.small_mesh_scene(0, 192, 108),
         "features": lambda: scenes.feature_scene(0, 160, 90),
         "features_seed4": lambda: scenes.feature_scene(4, 128, 72, max_depth=6),
+        "textured_ibl": lambda: scenes.small_textured_scene(0, 160, 90),
     }
 
 
@@ -87,7 +95,7 @@ def test_primary_hits_bit_exact(name):
 def test_render_matches_oracle(name, engine):
     native.set_render_options(engine=engine)
     w = workloads()[name]()
-    r = RayTracingRenderer(w.scene, max_depth=int(w.settings["max_depth"]))
+    r = renderer_for(w)
     pix, dep = r.render(Viewport(w.camera, w.width, w.height))
     opix, odep, _ = O.oracle_render(w.scene, w.projection(), w.settings, w.width, w.height, layout=L)
     assert_pixels_close(pix, opix, w.width, w.height)
@@ -140,3 +148,38 @@ def test_work_counters_match_oracle(engine):
         keys += ["scene_node_tests", "mesh_node_tests", "triangle_tests", "geometry_tests", "mesh_hit_fetches"]
     for k in keys:
         assert got[k] == ref[k], (k, got[k], ref[k])
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_ray_cone_mips_match_oracle(engine):
+    """SLIM_CONES_PER_PIXEL: mip levels chosen from the per-pixel cone spread
+    (the reference's intended ray cones) instead of its effective mip 0."""
+    native.set_render_options(engine=engine, ray_cones=L.CONES_PER_PIXEL)
+    try:
+        w = scenes.small_textured_scene(1, 160, 90)
+        r = renderer_for(w)
+        pix, dep = r.render(Viewport(w.camera, w.width, w.height))
+        # mip-level debug view must differ from mip 0 somewhere
+        r2 = RayTracingRenderer(w.scene, render_mode=L.RENDER_MIP_LEVEL)
+        mip, _ = r2.render(Viewport(w.camera, w.width, w.height))
+    finally:
+        native.set_render_options(engine=engine)
+    opix, odep, _ = O.oracle_render(w.scene, w.projection(), w.settings, w.width, w.height, layout=L,
+                                    cones_per_pixel=True)
+    assert_pixels_close(pix, opix, w.width, w.height)
+    assert_float_pixels_close(pix, opix)
+    st = L.default_settings(max_depth=3, render_mode=L.RENDER_MIP_LEVEL)
+    omip, _, _ = O.oracle_render(w.scene, w.projection(), st, w.width, w.height, layout=L, cones_per_pixel=True)
+    assert np.array_equal(mip.view(np.uint32), omip.view(np.uint32))
+    assert len(np.unique(omip[:, :3], axis=0)) > 2
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_normal_map_debug_mode(engine):
+    native.set_render_options(engine=engine)
+    w = scenes.small_textured_scene(2, 128, 72)
+    r = RayTracingRenderer(w.scene, render_mode=L.RENDER_NORMAL_MAP)
+    pix, dep = r.render(Viewport(w.camera, w.width, w.height))
+    st = L.default_settings(max_depth=3, render_mode=L.RENDER_NORMAL_MAP)
+    opix, _, _ = O.oracle_render(w.scene, w.projection(), st, w.width, w.height, layout=L)
+    assert np.array_equal(pix.view(np.uint32), opix.view(np.uint32))

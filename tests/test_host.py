@@ -171,3 +171,45 @@ def test_emissive_quad_flag():
     assert int(Scene(np.array(g), mats).data["flags"]) == L.SCENE_HAD_EMISSIVE_QUADS
     g[1]["material_id"] = 0
     assert int(Scene(np.array(g), mats).data["flags"]) == 0
+
+
+def _load_bmp_components(path):
+    """The component buffer the reference's loadBitmap returns
+    (platforms/win32_bitmap.h:122-160): raw B,G,R[,A] bytes, rows flipped to
+    top-down when the BMP is stored bottom-up."""
+    import struct
+    b = Path(path).read_bytes()
+    off = struct.unpack_from("<I", b, 10)[0]
+    w, h = struct.unpack_from("<ii", b, 18)
+    ch = 4 if struct.unpack_from("<H", b, 28)[0] == 32 else 3
+    comp = np.frombuffer(b, np.uint8, count=w * abs(h) * ch, offset=off).reshape(abs(h), w, ch)
+    return np.ascontiguousarray(comp[::-1] if h > 0 else comp)
+
+
+@pytest.mark.parametrize("name", ["cathedral_irradiance", "bolonga_irradiance"])
+def test_texture_baker_reproduces_shipped_reference_textures(name, tmp_path):
+    """The reference ships these cube maps baked by its bmp2texture -c -l
+    from the BMPs beside them; the restated baker must write the same bytes."""
+    from slimtracincpp_b200.scene import TextureAsset
+    ex = Path("/root/reference/src/examples")
+    if not (ex / f"{name}.texture").exists():
+        pytest.skip("reference assets not present")
+    t = TextureAsset.bake(_load_bmp_components(ex / f"{name}.bmp"), L.IMAGE_CUBEMAP | L.IMAGE_LINEAR)
+    t.save(tmp_path / "t.texture")
+    assert (tmp_path / "t.texture").read_bytes() == (ex / f"{name}.texture").read_bytes()
+    back = TextureAsset.load(ex / f"{name}.texture")
+    assert back.mip_sizes == [(512, 128), (128, 128), (128, 128)]
+
+
+def test_texture_round_trip_and_mip_chain(tmp_path):
+    from slimtracincpp_b200.scene import TextureAsset
+    rng = np.random.default_rng(0)
+    img = rng.integers(0, 256, (64, 64, 3), dtype=np.uint8)
+    t = TextureAsset.bake(img, L.IMAGE_MIPMAP | L.IMAGE_WRAP)
+    assert t.mip_sizes == [(64, 64), (32, 32), (16, 16), (8, 8), (4, 4)]
+    t.save(tmp_path / "a.texture")
+    back = TextureAsset.load(tmp_path / "a.texture")
+    assert back.quads.tobytes() == t.quads.tobytes() and back.mip_sizes == t.mip_sizes
+    # wrap: the border quads repeat the opposite edge
+    q = t.mip_quads(0)
+    assert q[0, 0]["R"][3] == q[0, 0]["R"][3]

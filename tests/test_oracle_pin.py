@@ -66,7 +66,8 @@ needs_ref = pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref 
     lambda: scenes.small_mesh_scene(3, 96, 54),
     lambda: scenes.feature_scene(1, 96, 54),
     lambda: scenes.feature_scene(2, 64, 36, max_depth=8),
-], ids=["config1", "config1_s5", "mesh", "features", "features_d8"])
+    lambda: scenes.small_textured_scene(3, 96, 54),
+], ids=["config1", "config1_s5", "mesh", "features", "features_d8", "textured_ibl"])
 def test_oracle_matches_reference_live(make):
     w = make()
     proj = w.projection()
@@ -77,9 +78,10 @@ def test_oracle_matches_reference_live(make):
 
 
 @needs_ref
-@pytest.mark.parametrize("mode", [L.RENDER_NORMALS, L.RENDER_DEPTH, L.RENDER_UVS, L.RENDER_MIP_LEVEL])
+@pytest.mark.parametrize("mode", [L.RENDER_NORMALS, L.RENDER_DEPTH, L.RENDER_UVS, L.RENDER_MIP_LEVEL,
+                                  L.RENDER_NORMAL_MAP])
 def test_oracle_debug_modes_match_reference(mode):
-    w = scenes.feature_scene(3, 64, 36)
+    w = scenes.small_textured_scene(3, 64, 36)
     st = L.default_settings(max_depth=4, render_mode=mode)
     proj = w.projection()
     rp, rd = O.reference_render(w.scene, proj, st, w.width, w.height, layout=L)

@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     p.add_argument("--seed", type=int, default=0)
-    p.add_argument("--config", default="config2", choices=["config1", "config2", "config3"],
+    p.add_argument("--config", default="config2", choices=["config1", "config2", "config3", "config4"],
                    help="workload (default: config2, the metric's 1080p mesh PBR scene)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
@@ -65,18 +65,52 @@ def dist_info():
     return rank, world, local
 
 
+def device_uuid(dev):
+    """NVML name of the CUDA device (CUDA_VISIBLE_DEVICES may renumber devices)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    NVML is polled from a thread every 2 ms (read-only queries), so even a
+    timed region of a few milliseconds gets samples; nvidia-smi -lms 200 is
+    the fallback when NVML cannot be loaded."""
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
              "clocks_event_reasons.sw_power_cap"
+    REASONS = [("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4)]
 
-    def __init__(self, index):
+    def __init__(self, index, uuid=None):
         self.index = index
+        self.uuid = uuid
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.samples = []
+        self.stop_flag = threading.Event()
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            if self.uuid:
+                self.handle = pynvml.nvmlDeviceGetHandleByUUID(self.uuid)
+            else:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -86,11 +120,29 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        p = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                mhz = p.nvmlDeviceGetClockInfo(self.handle, p.NVML_CLOCK_SM)
+                bits = p.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((float(mhz), int(bits)))
+            except Exception:
+                break
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sms = [m for m, _ in self.samples]
+            reasons = sorted({n for _, b in self.samples for n, bit in self.REASONS if b & bit})
+            return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": float(self.max_mhz),
+                    "reasons": reasons, "samples": len(sms), "source": "nvml, 2 ms polling"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -99,7 +151,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sms, maxes, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         for line in self.lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
@@ -113,7 +165,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
-                "reasons": sorted(reasons), "samples": len(sms)}
+                "reasons": sorted(reasons), "samples": len(sms), "source": "nvidia-smi -lms 200"}
 
 
 def algorithmic_bytes(w):
@@ -211,6 +263,179 @@ def run_reference(args):
     return 0
 
 
+NRC_FLOPS_PER_QUERY = 2 * (96 * 64 + 3 * 64 * 64 + 64 * 16)   # tensor-core MACs x 2 (output padded to 16)
+
+
+def timed_frames(torch, native, r, vp, sp, stream, outputs, flush):
+    """One device-resident frame (scene refit + render) per entry of
+    `outputs` (pixel, depth tensors), L2 flushed before each, timed with
+    CUDA events on the launching stream."""
+    lib = native.lib()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in outputs]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in outputs]
+    for i, (pix, dep) in enumerate(outputs):
+        flush.zero_()
+        starts[i].record(stream)
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, pix.data_ptr(), dep.data_ptr(), sp)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)]
+
+
+def run_cache_bench(args, torch, dist, dev, rank, world, local):
+    """Config 4: the config-2 scene at bounce depth 8.  Plain wavefront frames
+    against radiance-cache frames (paths stop at vertex 2, 65,536 training
+    paths and four Adam steps of 16,384 per frame, then the cache answers
+    every query); every timed cache frame is scored against the plain
+    depth-8 frame (PSNR of the 8-bit canvas, max abs of the stored values)."""
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200 import native, scenes
+    from slimtracincpp_b200.radiance_cache import RadianceCache
+    from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport, make_canvas
+    w = scenes.config4(args.seed)
+    lib = native.lib()
+    st = w.settings
+    r = RayTracingRenderer(w.scene, int(st["max_depth"]))
+    vp = Viewport(w.camera, w.width, w.height)
+    n = w.samples
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    steps = args.steps
+
+    def buffers(k):
+        return [(torch.empty((n, 4), dtype=torch.float32, device=dev), torch.empty(n, dtype=torch.float32, device=dev))
+                for _ in range(k)]
+
+    def counted(mode):
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, count_work=True, radiance_cache=mode)
+        out = buffers(1)
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, out[0][0].data_ptr(), out[0][1].data_ptr(), sp)
+        torch.cuda.synchronize()
+        wk = native.work_counters()
+        return wk["primary_rays"] + wk["shadow_rays"] + wk["bounce_rays"]
+
+    # plain depth-8 frames: timing and the reference image
+    plain_rays = counted(L.CACHE_OFF)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True)
+    ref = buffers(1)
+    for _ in range(args.warmup):
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, ref[0][0].data_ptr(), ref[0][1].data_ptr(), sp)
+    native.reset_stage_stats()
+    plain_ms = timed_frames(torch, native, r, vp, sp, stream, ref * steps, flush)
+    plain_stages = {s["name"]: s["total_ms"] / steps for s in native.stage_stats() if s["launches"]}
+
+    # radiance-cache frames (online training continues through warm-up and timing)
+    cache = RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=args.seed)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True, radiance_cache=L.CACHE_ON)
+    outs = buffers(steps)
+    for _ in range(args.warmup):
+        native.check(lib.slimRefitSceneBVH(sp))
+        r.render_to_device(vp, outs[0][0].data_ptr(), outs[0][1].data_ptr(), sp)
+    torch.cuda.synchronize()
+    native.reset_stage_stats()
+    clocks = ClockSampler(local, device_uuid(dev))
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    cache_ms = timed_frames(torch, native, r, vp, sp, stream, outs, flush)
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    stats = {s["name"]: s for s in native.stage_stats()}
+    cstats = cache.stats()
+
+    # per-frame quality against the plain depth-8 frame
+    ref_pix = ref[0][0]
+    ref8 = torch.floor(255.0 * torch.sqrt(ref_pix[:, :3].clamp(0, 1)))
+    psnr, max_abs = [], []
+    for pix, _ in outs:
+        p8 = torch.floor(255.0 * torch.sqrt(pix[:, :3].clamp(0, 1)))
+        mse = float(((p8 - ref8) ** 2).mean())
+        psnr.append(99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse))
+        max_abs.append(float((pix[:, :3] - ref_pix[:, :3]).abs().max()))
+    cache_rays = counted(L.CACHE_ON)
+
+    # end to end through the C ABI with host buffers, cache on
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
+    pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    pin_geo = torch.empty(w.scene.geometries.nbytes, dtype=torch.uint8, pin_memory=True)
+    pin_geo.numpy().view(L.GEOMETRY)[:] = w.scene.geometries
+    sd = w.scene.data.copy()
+    sd["geometries"] = pin_geo.data_ptr()
+    cv, _, _ = make_canvas(w.width, w.height, L.AA_NONE)
+    cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
+    proj = w.projection()
+    for _ in range(args.warmup):
+        native.check(lib.slimUploadGeometries(native.ptr(sd)))
+        native.check(lib.slimRefitSceneBVH(None))
+        native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        native.check(lib.slimUploadGeometries(native.ptr(sd)))
+        native.check(lib.slimRefitSceneBVH(None))
+        native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
+    e2e_s = time.perf_counter() - t0
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+
+    times = torch.tensor([sum(cache_ms), sum(plain_ms), e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    cache_total, plain_total, e2e_s = float(times[0]), float(times[1]), float(times[2])
+    value = cache_rays * steps * world / (cache_total / 1000.0) / 1e6
+    timed = {k: v for k, v in stats.items() if v["launches"]}
+    stages = {k: v["total_ms"] / steps for k, v in timed.items()}
+    q = stats.get("cache_query")
+    nrc_roofline = None
+    if q and q["launches"]:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        peak_tf = float(peaks.get("bf16_tflops", 1590.0))
+        ach = cstats["queries"] * NRC_FLOPS_PER_QUERY / (q["total_ms"] / q["launches"] / 1000.0) / 1e12
+        nrc_roofline = {"kernel": "k_nrc_infer", "bound": "tensor", "achieved": ach, "peak": peak_tf,
+                        "unit": "TFLOP/s", "frac": ach / peak_tf, "flops_per_query": NRC_FLOPS_PER_QUERY,
+                        "queries": cstats["queries"], "ms_per_launch": q["total_ms"] / q["launches"],
+                        "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops)" if peaks else "fallback"}
+    dom = max(timed, key=lambda k: timed[k]["total_ms"]) if timed else None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": cache_total / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded config2 scene, depth 8)",
+            "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 8, "cache_depth": 2,
+                       "train_samples_per_frame": 65536, "batch": 16384, "learning_rate": 1e-2,
+                       "engine": "wavefront", "parallelism": f"replicas x{world}",
+                       "l2": "flushed between steps (512 MiB write)", "rays_per_frame": cache_rays},
+            "ms_per_frame": cache_total / steps,
+            "plain_depth8": {"ms_per_frame": plain_total / steps, "rays_per_frame": plain_rays,
+                             "mrays_s": plain_rays * steps * world / (plain_total / 1000.0) / 1e6,
+                             "stages_ms_per_frame": plain_stages},
+            "speedup_vs_plain_depth8": plain_total / cache_total,
+            "psnr_db_per_frame": psnr, "max_abs_per_frame": max_abs,
+            "cache": {"queries": cstats["queries"], "train_samples": cstats["train_samples"],
+                      "loss": cstats["loss"], "steps": cstats["steps"], "frames": cstats["frames"]},
+            "stages_ms_per_frame": stages, "dominant_stage": dom,
+            "roofline": nrc_roofline,
+            "e2e": {"value": cache_rays * steps * world / e2e_s / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": int(w.scene.geometries.nbytes),
+                    "d2h_bytes_per_step": int(pin_pix.numel() * 4 + pin_dep.numel() * 4),
+                    "ms_per_step": 1000.0 * e2e_s / steps},
+            "clocks": clock_info,
+            "gpu_launches": None}
+    # our kernels per cache frame: trace stages + cache stages (train = 2 kernels per step)
+    per_frame = 0
+    for k, v in stats.items():
+        per_frame += v["launches"] * (2 if k == "refit" else 8 if k == "cache_train" else 1)
+    line["gpu_launches"] = per_frame
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -223,6 +448,8 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.config == "config4":
+        return run_cache_bench(args, torch, dist, dev, rank, world, local)
 
     from slimtracincpp_b200 import layout as L
     from slimtracincpp_b200 import native, scenes
@@ -267,7 +494,7 @@ def main():
         r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
     torch.cuda.synchronize()
     native.reset_stage_stats()
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, device_uuid(dev))
     clocks.start()
     if world > 1:
         dist.barrier()

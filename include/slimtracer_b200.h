@@ -35,6 +35,7 @@ extern "C" {
 #define SLIM_ERR_LIMIT       4   /* a fixed capacity would be exceeded       */
 #define SLIM_ERR_IO          5   /* file missing, truncated or malformed     */
 #define SLIM_ERR_STACK       6   /* a traversal stack overflowed (device)    */
+#define SLIM_ERR_TIMEOUT     7   /* a bounded device wait gave up            */
 
 /* ---- enums and flags (core/base.h:137-149,402-414,626-633,655-660) ----- */
 enum { SLIM_GEOMETRY_NONE = 0, SLIM_GEOMETRY_MESH, SLIM_GEOMETRY_GRID, SLIM_GEOMETRY_BOX,
@@ -186,14 +187,21 @@ enum { SLIM_SCENE_BVH_UPLOADED = 0, SLIM_SCENE_BVH_REFIT = 1 };
 typedef struct {
     int32_t engine;          /* SLIM_ENGINE_*: wavefront queues (default) or one fused kernel */
     int32_t ray_cones;       /* SLIM_CONES_REFERENCE (default): the reference's effective ray
-                                cone (mip 0, see DESIGN); SLIM_CONES_PER_PIXEL: per-pixel spread */
+                                cone (mip 0: its copy of the aux hit clears the per-pixel
+                                spread); SLIM_CONES_PER_PIXEL: per-pixel spread */
     int32_t scene_bvh;       /* SLIM_SCENE_BVH_UPLOADED (default) or GPU refit of its topology */
     int32_t block_size;      /* threads per block, 0 = tuned default */
     int32_t count_work;      /* non-zero: accumulate per-frame work counters (slower) */
     int32_t profile_stages;  /* non-zero: time every stage launch with CUDA events */
     int32_t shadow_queue_mb; /* wavefront shadow-ray queue budget in MiB, 0 = 1024 */
-    int32_t _reserved;
+    int32_t radiance_cache;  /* SLIM_CACHE_*: with the wavefront engine and a configured
+                                radiance cache, paths stop at the cache depth and take the
+                                cache's answer.  OFF (default); ON: the network; TRUNCATE:
+                                nothing (the method without the network); EXACT: every
+                                query traced on to max_depth by the tracer (a check of the
+                                cache plumbing: equals the plain frame up to rounding) */
 } SlimRenderOptions;
+enum { SLIM_CACHE_OFF = 0, SLIM_CACHE_ON = 1, SLIM_CACHE_TRUNCATE = 2, SLIM_CACHE_EXACT = 3 };
 
 /* Work counters of the last frame (rays traced and memory records touched). */
 typedef struct {
@@ -313,6 +321,53 @@ int slimResetStageStats(void);
  * (GPU), keeping the topology last uploaded: scene/scene.h:165-191 rebuilds
  * it from scratch on the host every frame instead. */
 int slimRefitSceneBVH(void *stream);
+
+/* ---- Neural radiance cache.  No counterpart in the reference. ----------
+ * A 96-64-64-64-64-3 MLP (ReLU, exp output; bf16 weights and activations,
+ * f32 accumulation on the sm_100a tensor cores) that stands in for the rest
+ * of a path from the cache depth on.  Inputs per sample, 16 floats:
+ *   (p.xyz, roughness) (direction.xyz, 0) (normal.xyz, 0) (albedo.xyz, 0)
+ * with p the hit position mapped to [0,1]^3 by the scene box.  It is
+ * encoded as 12-octave sin/cos of p, bands 0..3 spherical harmonics of the
+ * direction, normal, roughness, albedo and a constant 1.  Parameters: one
+ * f32 vector of SLIM_NRC_PARAMS, W0 [64][96], W1..W3 [64][64], W4 [3][64]
+ * (row = output unit).  Training: relative L2 loss, Adam. */
+#define SLIM_NRC_PARAMS 18624
+#define SLIM_NRC_FEATURES 16
+typedef struct {
+    uint32_t cache_depth;    /* path vertex the cache answers at (>= 2) */
+    uint32_t train_samples;  /* training paths per frame (65536) */
+    uint32_t batch;          /* samples per Adam step (16384) */
+    uint32_t seed;           /* weight initialisation, per-frame sample selection */
+    float learning_rate;     /* 1e-2 */
+    float beta1, beta2, epsilon;   /* 0.9, 0.99, 1e-8 */
+    uint32_t train;          /* non-zero: train online every rendered frame */
+    uint32_t _reserved[3];
+} SlimRadianceCacheConfig;
+typedef struct {
+    uint64_t frames, steps;  /* frames rendered with the cache, Adam steps taken */
+    uint32_t queries;        /* cache queries of the last frame */
+    uint32_t train_samples;  /* training samples of the last frame */
+    float loss;              /* mean relative-L2 loss of the last step */
+    float _pad;
+} SlimRadianceCacheStats;
+
+/* Allocates the cache (needs slimInitDataOnGPU), initialises the weights
+ * from config->seed and clears the Adam state. */
+int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config);
+int slimRadianceCacheGetConfig(SlimRadianceCacheConfig *config);
+/* f32 master weights (host arrays of SLIM_NRC_PARAMS); setting them clears
+ * the Adam moments and step count. */
+int slimRadianceCacheSetWeights(const float *params, uint32_t count);
+int slimRadianceCacheGetWeights(float *params, uint32_t count);
+/* Mean-loss gradient of the last training step. */
+int slimRadianceCacheGetGradients(float *grad, uint32_t count);
+/* Device pointers: radiance (float4 per sample, rgb) of `count` samples of
+ * SLIM_NRC_FEATURES floats.  Asynchronous on `stream`. */
+int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radiance, void *stream);
+/* One Adam step over `count` (features, target float4 rgb) device samples. */
+int slimRadianceCacheTrain(const void *d_features, const void *d_targets, uint32_t count, void *stream);
+int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats);
 
 /* Host-side helpers: the reference's own host algorithms, restated. */
 

@@ -2,6 +2,7 @@
 // plus the device-resident extensions.  One process-wide render context,
 // like the reference's module-global GPU mirror (renderer/renderer_GPU.h:
 // 12-20); calls are serialised by a mutex.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -14,6 +15,7 @@
 #include "device_scene.h"
 #include "host_common.h"
 #include "kernels.h"
+#include "nrc.h"
 
 namespace slim {
 
@@ -84,6 +86,31 @@ struct Context {
     DevArray<unsigned long long> w_shadow_mask;
     DevArray<float4> w_pairs;
     struct EventTimer *timer = nullptr;
+
+    // neural radiance cache
+    struct Cache : CacheTrainer {
+        bool configured = false;
+        SlimRadianceCacheConfig config{};
+        DevArray<float> params, m, v, grad, partials, loss_partials, loss;
+        DevArray<uint8_t> image;
+        DevArray<float4> features, aux, radiance, t_features, t_targets, t_color, t_through;
+        DevArray<uint32_t> counts;
+        uint32_t *error_flags = nullptr;
+        uint64_t steps = 0, frames = 0;
+        cudaError_t step(const float4 *f, const float4 *t, uint32_t samples, const uint32_t *count, uint32_t offset,
+                         cudaStream_t stream) override {
+            steps++;
+            nrc::AdamArgs a{};
+            a.lr = config.learning_rate;
+            a.beta1 = config.beta1;
+            a.beta2 = config.beta2;
+            a.eps = config.epsilon;
+            a.bias1 = (float)(1.0 / (1.0 - std::pow((double)config.beta1, (double)steps)));
+            a.bias2 = (float)(1.0 / (1.0 - std::pow((double)config.beta2, (double)steps)));
+            return nrc::launch_train_step(f, t, samples, count, offset, params.ptr, m.ptr, v.ptr, image.ptr,
+                                          partials.ptr, loss_partials.ptr, grad.ptr, loss.ptr, a, error_flags, stream);
+        }
+    } cache;
 };
 
 // CUDA-event pairs around stage launches, resolved lazily.
@@ -128,7 +155,8 @@ struct EventTimer : StageTimer {
         for (int i = 0; i < STAGE_COUNT; i++) { launches[i] = 0; total_ms[i] = 0; }
     }
 };
-const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit", "shadow_mesh"};
+const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit", "shadow_mesh",
+                                        "cache", "cache_train", "cache_query"};
 SlimWorkCounters g_stage_work[STAGE_COUNT];
 
 Context g_ctx;
@@ -475,6 +503,48 @@ int check_settings(const Context &c, const SlimRayTracerSettings *st) {
 
 int ensure_wavefront(Context &c, uint32_t samples);
 
+// Buffers and per-frame parameters of a radiance-cache frame.
+int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
+    Context::Cache &k = c.cache;
+    if (!k.configured) return set_error(SLIM_ERR_STATE, "radiance_cache is set but slimRadianceCacheConfigure was not called");
+    const int mode = c.options.radiance_cache;
+    const uint32_t cap = mode == SLIM_CACHE_EXACT ? samples : k.config.train_samples;
+    int rc;
+    if ((rc = k.features.reserve(4 * (size_t)samples, "alloc cache queries"))) return rc;
+    if ((rc = k.aux.reserve(2 * (size_t)samples, "alloc cache query rays"))) return rc;
+    if ((rc = k.radiance.reserve(samples, "alloc cache answers"))) return rc;
+    if ((rc = k.counts.reserve(2, "alloc cache counters"))) return rc;
+    if (cap) {
+        if ((rc = k.t_targets.reserve(cap, "alloc training targets"))) return rc;
+        if ((rc = k.t_color.reserve(cap, "alloc training paths"))) return rc;
+        if ((rc = k.t_through.reserve(cap, "alloc training paths"))) return rc;
+        if (mode == SLIM_CACHE_ON && (rc = k.t_features.reserve(4 * (size_t)cap, "alloc training samples"))) return rc;
+    }
+    cf.mode = mode;
+    cf.depth = k.config.cache_depth;
+    cf.features = k.features.ptr;
+    cf.aux = k.aux.ptr;
+    cf.radiance = k.radiance.ptr;
+    cf.counts = k.counts.ptr;
+    cf.train_capacity = cap;
+    cf.t_features = k.t_features.ptr;
+    cf.t_targets = k.t_targets.ptr;
+    cf.t_color = k.t_color.ptr;
+    cf.t_through = k.t_through.ptr;
+    // stratified selection offset of this frame (SplitMix64 of seed and frame)
+    uint64_t z = ((uint64_t)k.config.seed << 32) + k.frames + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    cf.select_offset = (float)((z >> 40) * (1.0 / 16777216.0));
+    cf.batch = k.config.batch;
+    cf.weights = k.image.ptr;
+    cf.trainer = (mode == SLIM_CACHE_ON && k.config.train) ? &k : nullptr;
+    k.error_flags = c.d_error.ptr;
+    k.frames++;
+    return SLIM_OK;
+}
+
 StageTimer *timer_for(Context &c) {
     if (!c.options.profile_stages) return nullptr;
     if (!c.timer) c.timer = new EventTimer();
@@ -513,7 +583,13 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     } else {
         rc = ensure_wavefront(c, F.width * F.height);
         if (rc) return rc;
-        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream, timer);
+        CacheFrame cf;
+        const CacheFrame *cache = nullptr;
+        if (c.options.radiance_cache != SLIM_CACHE_OFF) {
+            if ((rc = cache_frame(c, F.width * F.height, cf))) return rc;
+            cache = &cf;
+        }
+        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream, timer, cache);
     }
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return SLIM_OK;
@@ -571,6 +647,7 @@ int read_errors(Context &c, cudaStream_t stream) {
     if (flags) {
         SLIM_CUDA(cudaMemset(c.d_error.ptr, 0, 4), "clear error flags");
         if (flags & kErrStack) return set_error(SLIM_ERR_STACK, "a traversal stack overflowed on the device");
+        if (flags & nrc::kErrTimeout) return set_error(SLIM_ERR_TIMEOUT, "a tensor-core wait timed out on the device");
         return set_error(SLIM_ERR_STATE, "device reported an index error");
     }
     return SLIM_OK;
@@ -734,7 +811,8 @@ int slimSetRenderOptions(const SlimRenderOptions *options) {
     if (!options) return set_error(SLIM_ERR_ARGUMENT, "options is null");
     if (options->engine < 0 || options->engine > 1 || options->ray_cones < 0 || options->ray_cones > 1 ||
         options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 1024 ||
-        (options->block_size % 32))
+        (options->block_size % 32) || options->radiance_cache < SLIM_CACHE_OFF ||
+        options->radiance_cache > SLIM_CACHE_EXACT)
         return set_error(SLIM_ERR_ARGUMENT, "bad render options");
     g_ctx.options = *options;
     return SLIM_OK;
@@ -936,3 +1014,167 @@ extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const Sli
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc render launch");
     return SLIM_OK;
 }
+
+// ---- neural radiance cache --------------------------------------------------
+namespace {
+
+uint64_t splitmix64(uint64_t &state) {
+    uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// He-uniform weights (bound sqrt(6 / fan_in)); the output layer 10x smaller,
+// so the untrained cache answers about exp(0) = 1.
+void init_cache_weights(uint32_t seed, std::vector<float> &w) {
+    w.assign(nrc::kParams, 0.0f);
+    uint64_t state = 0x5EEDull ^ ((uint64_t)seed << 17);
+    const int rows[5] = {nrc::kHidden, nrc::kHidden, nrc::kHidden, nrc::kHidden, nrc::kOutputs};
+    const int cols[5] = {nrc::kInputs, nrc::kHidden, nrc::kHidden, nrc::kHidden, nrc::kHidden};
+    size_t o = 0;
+    for (int l = 0; l < 5; l++) {
+        double bound = std::sqrt(6.0 / cols[l]) * (l == 4 ? 0.1 : 1.0);
+        for (int i = 0; i < rows[l] * cols[l]; i++) {
+            double u = (double)(splitmix64(state) >> 11) * (1.0 / 9007199254740992.0);
+            w[o++] = (float)((2.0 * u - 1.0) * bound);
+        }
+    }
+}
+
+int cache_sync_errors(Context &c) {
+    SLIM_CUDA(cudaDeviceSynchronize(), "radiance cache");
+    return read_errors(c, nullptr);
+}
+
+int upload_cache_weights(Context &c, const float *params) {
+    Context::Cache &k = c.cache;
+    SLIM_CUDA(cudaMemcpy(k.params.ptr, params, nrc::kParams * sizeof(float), cudaMemcpyHostToDevice), "upload weights");
+    SLIM_CUDA(cudaMemset(k.m.ptr, 0, nrc::kParams * sizeof(float)), "clear adam");
+    SLIM_CUDA(cudaMemset(k.v.ptr, 0, nrc::kParams * sizeof(float)), "clear adam");
+    SLIM_CUDA(cudaMemset(k.grad.ptr, 0, nrc::kParams * sizeof(float)), "clear gradient");
+    SLIM_CUDA(cudaMemset(k.loss.ptr, 0, sizeof(float)), "clear loss");
+    SLIM_CUDA(nrc::launch_pack_weights(k.params.ptr, k.image.ptr, nullptr), "pack weights");
+    k.steps = 0;
+    return cache_sync_errors(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!config) return set_error(SLIM_ERR_ARGUMENT, "config is null");
+    const SlimRadianceCacheConfig &k = *config;
+    if (k.cache_depth < 2 || k.cache_depth > 255 || !k.batch || !(k.learning_rate > 0.0f) || !(k.beta1 >= 0.0f) ||
+        !(k.beta1 < 1.0f) || !(k.beta2 >= 0.0f) || !(k.beta2 < 1.0f) || !(k.epsilon > 0.0f) ||
+        k.train_samples > (1u << 26))
+        return set_error(SLIM_ERR_ARGUMENT, "bad radiance cache config");
+    Context::Cache &st = c.cache;
+    int rc;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    if ((rc = st.params.reserve(nrc::kParams, "alloc cache weights"))) return rc;
+    if ((rc = st.m.reserve(nrc::kParams, "alloc adam"))) return rc;
+    if ((rc = st.v.reserve(nrc::kParams, "alloc adam"))) return rc;
+    if ((rc = st.grad.reserve(nrc::kParams, "alloc gradient"))) return rc;
+    if ((rc = st.partials.reserve((size_t)sms * nrc::kParams, "alloc partial gradients"))) return rc;
+    if ((rc = st.loss_partials.reserve((size_t)sms, "alloc partial losses"))) return rc;
+    if ((rc = st.loss.reserve(1, "alloc loss"))) return rc;
+    if ((rc = st.image.reserve(nrc::kImgBytes, "alloc weight image"))) return rc;
+    st.config = k;
+    st.frames = 0;
+    st.error_flags = c.d_error.ptr;
+    std::vector<float> w;
+    init_cache_weights(k.seed, w);
+    if ((rc = upload_cache_weights(c, w.data()))) return rc;
+    st.configured = true;
+    return SLIM_OK;
+}
+
+int slimRadianceCacheGetConfig(SlimRadianceCacheConfig *config) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!config) return set_error(SLIM_ERR_ARGUMENT, "config is null");
+    if (!g_ctx.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    *config = g_ctx.cache.config;
+    return SLIM_OK;
+}
+
+int slimRadianceCacheSetWeights(const float *params, uint32_t count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if (!params || count != (uint32_t)nrc::kParams) return set_error(SLIM_ERR_ARGUMENT, "expected SLIM_NRC_PARAMS weights");
+    return upload_cache_weights(c, params);
+}
+
+int slimRadianceCacheGetWeights(float *params, uint32_t count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if (!params || count != (uint32_t)nrc::kParams) return set_error(SLIM_ERR_ARGUMENT, "expected SLIM_NRC_PARAMS weights");
+    int rc = cache_sync_errors(c);
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(params, c.cache.params.ptr, nrc::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read weights");
+    return SLIM_OK;
+}
+
+int slimRadianceCacheGetGradients(float *grad, uint32_t count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if (!grad || count != (uint32_t)nrc::kParams) return set_error(SLIM_ERR_ARGUMENT, "expected SLIM_NRC_PARAMS values");
+    int rc = cache_sync_errors(c);
+    if (rc) return rc;
+    SLIM_CUDA(cudaMemcpy(grad, c.cache.grad.ptr, nrc::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read gradient");
+    return SLIM_OK;
+}
+
+int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radiance, void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if ((!d_features || !d_radiance) && count) return set_error(SLIM_ERR_ARGUMENT, "null device buffer");
+    cudaError_t e = nrc::launch_infer((const float4 *)d_features, nullptr, count, count, (float4 *)d_radiance,
+                                      c.cache.image.ptr, c.d_error.ptr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cache query launch");
+    return SLIM_OK;
+}
+
+int slimRadianceCacheTrain(const void *d_features, const void *d_targets, uint32_t count, void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if ((!d_features || !d_targets) && count) return set_error(SLIM_ERR_ARGUMENT, "null device buffer");
+    if (!count) return SLIM_OK;
+    c.cache.error_flags = c.d_error.ptr;
+    cudaError_t e = c.cache.step((const float4 *)d_features, (const float4 *)d_targets, count, nullptr, 0,
+                                 (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cache train launch");
+    return SLIM_OK;
+}
+
+int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!stats) return set_error(SLIM_ERR_ARGUMENT, "stats is null");
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    int rc = cache_sync_errors(c);
+    if (rc) return rc;
+    memset(stats, 0, sizeof(*stats));
+    stats->frames = c.cache.frames;
+    stats->steps = c.cache.steps;
+    SLIM_CUDA(cudaMemcpy(&stats->loss, c.cache.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost), "read loss");
+    if (c.cache.counts.ptr) {
+        uint32_t counts[2] = {0, 0};
+        SLIM_CUDA(cudaMemcpy(counts, c.cache.counts.ptr, sizeof(counts), cudaMemcpyDeviceToHost), "read cache counts");
+        stats->queries = counts[0];
+        stats->train_samples = counts[1];
+    }
+    return SLIM_OK;
+}
+
+}  // extern "C"

@@ -8,7 +8,8 @@ namespace slim {
 // Stages of a frame, for per-stage timing and work counters (16 counter
 // slots per stage in DevFrame::counters).
 enum Stage : int {
-    STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_SHADOW_MESH, STAGE_COUNT
+    STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_SHADOW_MESH,
+    STAGE_CACHE, STAGE_CACHE_TRAIN, STAGE_CACHE_QUERY, STAGE_COUNT
 };
 constexpr int kCountersPerStage = 16;
 
@@ -33,7 +34,7 @@ struct WavefrontBuffers {
     float4 *path_color;              // per sample: accumulated colour (xyz), depth (w)
     float4 *path_throughput;         // per sample: throughput (xyz)
     float4 *rays[2];                 // ping-pong ray queues, 2 float4 per ray
-    uint32_t *queue_count;           // [0..1] ray queues, [2] shadow queue, [3] pairs, [4] pair cursor
+    uint32_t *queue_count;           // [0..1] ray queues, [2] shadow queue, [3] pairs, [4] pair cursor (8 slots)
     float4 *hits;                    // 3 float4 per queue slot
     float4 *shadow_rays;             // 2 float4 per shadow ray
     unsigned long long *shadow_mask; // per queue slot: occluded-light bits
@@ -42,8 +43,37 @@ struct WavefrontBuffers {
     uint32_t shadow_capacity;        // shadow ray slots
     uint32_t pair_capacity;          // candidate pair slots
 };
+
+// Radiance cache in a wavefront frame (no counterpart in the reference).
+// Paths stop at vertex `depth`: misses and emissive hits there finish as
+// usual, every other hit becomes a query whose answer -- the network's
+// (ON), nothing (TRUNCATE) or the tracer's own full-depth continuation
+// (EXACT, a check of the plumbing) -- is added with the path throughput.
+// With ON and a trainer, `train_capacity` queries (stratified over all of
+// them) are traced on to max_depth from the same vertex; their radiance is
+// the training target of the frame's Adam steps.
+struct CacheTrainer {
+    virtual cudaError_t step(const float4 *features, const float4 *targets, uint32_t samples, const uint32_t *count,
+                             uint32_t offset, cudaStream_t stream) = 0;
+    virtual ~CacheTrainer() = default;
+};
+struct CacheFrame {
+    int mode = 0;                  // SLIM_CACHE_*
+    uint32_t depth = 0;            // path vertex the cache answers at (>= 2)
+    float4 *features = nullptr;    // 4 per query (capacity: one per sample)
+    float4 *aux = nullptr;         // 2 per query: (ray origin, pixel) (ray direction, cone pixel)
+    float4 *radiance = nullptr;    // 1 per query
+    uint32_t *counts = nullptr;    // [0] queries, [1] training paths
+    uint32_t train_capacity = 0;   // training paths per frame (every query in EXACT mode)
+    float4 *t_features = nullptr, *t_targets = nullptr, *t_color = nullptr, *t_through = nullptr;
+    float select_offset = 0.0f;    // stratified selection offset in [0,1)
+    uint32_t batch = 0;            // samples per training step
+    const uint8_t *weights = nullptr;   // bf16 weight image
+    CacheTrainer *trainer = nullptr;    // null: no training this frame
+};
+
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream, StageTimer *timer);
+                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache = nullptr);
 
 // GPU refit of the scene BVH: recomputes every node's bounds bottom-up from
 // the geometries' world AABBs, keeping the uploaded topology.

@@ -20,6 +20,7 @@
 // the reference's order from the occlusion bits, so every colour is summed
 // in the same order as the reference's per-pixel loop.
 #include "kernels.h"
+#include "nrc.h"
 #include "tracer_core.cuh"
 
 namespace slim {
@@ -98,6 +99,10 @@ struct QueueArgs {
     uint32_t depth;               // 1-based bounce of this round
     uint32_t light_begin, light_end;
     unsigned long long *counters; // this stage's counter slots, or null
+    // radiance cache
+    float4 *sink;                 // non-null: finished paths write their linear colour here
+                                  // (indexed by the path slot) instead of the canvas
+    uint32_t skip_glow_depth;     // no light glow on the segment of this depth (0 = none)
 };
 
 SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
@@ -107,9 +112,13 @@ SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
     d = normalized(primary_direction(P, x, y));
 }
 
-SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel) {
+// `pixel` indexes the path state (and the canvas); `cone_pixel` is the canvas
+// pixel whose ray-cone spread the path uses.  They differ only for the
+// radiance cache's training paths, whose state lives in their own slots.
+SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel,
+                     uint32_t &cone_pixel) {
     if (!A.rays_in) {
-        pixel = slot;
+        pixel = cone_pixel = slot;
         primary_ray(F, slot, o, d);
         return;
     }
@@ -117,6 +126,15 @@ SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float
     o = xyz(a);
     pixel = __float_as_uint(a.w);
     d = xyz(b);
+    cone_pixel = __float_as_uint(b.w);
+}
+SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel) {
+    uint32_t cone_pixel;
+    load_ray(F, A, slot, o, d, pixel, cone_pixel);
+}
+SLIM_D float cone_scaling(const DevFrame &F, uint32_t cone_pixel) {
+    return F.cones_per_pixel ? pixel_scaling(F.projection, (int)(cone_pixel % F.width), (int)(cone_pixel / F.width))
+                             : 0.0f;
 }
 
 SLIM_D uint32_t queue_size(const QueueArgs &A) { return A.count_in ? *A.count_in : A.samples; }
@@ -159,8 +177,8 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, Queu
         if (live) {
             if (A.light_begin == 0) A.masks[slot] = 0ull;
             float3 o, d;
-            uint32_t pixel;
-            load_ray(F, A, slot, o, d, pixel);
+            uint32_t pixel, cone_pixel;
+            load_ray(F, A, slot, o, d, pixel, cone_pixel);
             Hit hit;
             int g = load_hit(A.hits, slot, hit);
             if (g >= 0) {
@@ -169,8 +187,7 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, Queu
                 if (!((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind)) {
                     Ray ray;
                     reset(ray, scale_add(d, kTraceOffset, o), d);
-                    float scaling = F.cones_per_pixel ? pixel_scaling(F.projection, (int)(pixel % F.width), (int)(pixel / F.width)) : 0.0f;
-                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
                     shaded = true;
                 }
             }
@@ -428,11 +445,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs
     for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
         bool live = slot < n;
         bool bounce = false;
-        uint32_t pixel = 0;
+        uint32_t pixel = 0, cone_pixel = 0;
         float3 bo = f3(0, 0, 0), bd = f3(0, 0, 0);
         if (live) {
             float3 o, d;
-            load_ray(F, A, slot, o, d, pixel);
+            load_ray(F, A, slot, o, d, pixel, cone_pixel);
             Ray ray;
             reset(ray, scale_add(d, kTraceOffset, o), d);
             Hit hit;
@@ -450,8 +467,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs
                     current = m.emission;
                 } else {
                     Surface s;
-                    float scaling = F.cones_per_pixel ? pixel_scaling(F.projection, (int)(pixel % F.width), (int)(pixel / F.width)) : 0.0f;
-                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
                     hit_distance = hit.distance;
                     if (A.depth == 1) depth = depth_at(F.projection, hit.position);
                     unsigned long long occluded = A.masks[slot];
@@ -482,12 +498,14 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs
             } else if (st.skybox_color_texture_id >= 0) {
                 current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
             }
-            add_glow(S, ray, hit_distance, current);
+            if (A.depth != A.skip_glow_depth) add_glow(S, ray, hit_distance, current);
             color = mul_add(current, throughput, color);
             throughput = throughput * next_throughput;
             if (bounce) {
                 A.path_color[pixel] = make_float4(color.x, color.y, color.z, depth);
                 A.path_throughput[pixel] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+            } else if (A.sink) {
+                A.sink[pixel] = make_float4(color.x, color.y, color.z, 0.0f);
             } else {
                 float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
                 set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, depth);
@@ -497,15 +515,147 @@ __global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs
         if (bounce) {
             bump<COUNT>(w.bounce);
             A.rays_out[2 * (size_t)q] = make_float4(bo.x, bo.y, bo.z, __uint_as_float(pixel));
-            A.rays_out[2 * (size_t)q + 1] = make_float4(bd.x, bd.y, bd.z, 0.0f);
+            A.rays_out[2 * (size_t)q + 1] = make_float4(bd.x, bd.y, bd.z, __uint_as_float(cone_pixel));
         }
     }
     flush_stage<COUNT>(A.counters, w);
 }
 
+// ---- radiance cache ----------------------------------------------------------
+struct CacheArgs {
+    float4 *features, *aux, *radiance;
+    uint32_t *count;               // queries
+    uint32_t *train_count;         // training paths
+    uint32_t train_capacity;
+    float4 *t_features, *t_targets, *t_color, *t_through;
+    float offset;
+    int mode;
+};
+
+// Vertex-`depth` hits of the main paths.  Misses and emissive quads finish the
+// path exactly as k_shade does; every other hit becomes a cache query: the
+// segment's glow is added to the path colour now, the surface's features are
+// appended for the network, and the path waits in path_color /
+// path_throughput for the answer.
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, QueueArgs A, CacheArgs C) {
+    uint32_t n = queue_size(A);
+    const SlimRayTracerSettings &st = F.settings;
+    Work w = {};
+    // scene box -> [0,1]^3 (longest side), from the scene BVH root
+    float4 r0 = make_float4(0, 0, 0, 1), r1 = make_float4(1, 1, 0, 0);
+    if (S.scene_node_count) { r0 = S.scene_nodes[0]; r1 = S.scene_nodes[1]; }
+    const float3 bmin = f3(r0.x, r0.y, r0.z);
+    const float ext = fmaxf(fmaxf(r0.w - r0.x, r1.x - r0.y), r1.y - r0.z);
+    const float inv = ext > 0.0f ? 1.0f / ext : 1.0f;
+    uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t rounds = (n + stride - 1) / stride;
+    for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
+        bool query = false;
+        uint32_t pixel = 0, cone_pixel = 0;
+        float3 o = f3(0, 0, 0), d = f3(0, 0, 0);
+        float4 f0 = make_float4(0, 0, 0, 0), f1 = f0, f2 = f0, f3v = f0;
+        if (slot < n) {
+            load_ray(F, A, slot, o, d, pixel, cone_pixel);
+            Ray ray;
+            reset(ray, scale_add(d, kTraceOffset, o), d);
+            Hit hit;
+            int g = load_hit(A.hits, slot, hit);
+            float4 pc = A.path_color[pixel];
+            float3 color = xyz(pc), throughput = xyz(A.path_throughput[pixel]);
+            float3 current = f3(0, 0, 0);
+            float hit_distance = INFINITY;
+            if (g >= 0) {
+                hit_distance = hit.distance;
+                Geo geo = load_geo(S, (uint32_t)g);
+                Mat m = load_mat(S, geo.material);
+                if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+                    current = m.emission;
+                } else {
+                    Surface s;
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
+                    hit_distance = hit.distance;
+                    query = true;
+                    float3 p = (s.P - bmin) * inv;
+                    float3 al = m.albedo * s.albedo_from_map;
+                    f0 = make_float4(p.x, p.y, p.z, m.roughness);
+                    f1 = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
+                    f2 = make_float4(s.N.x, s.N.y, s.N.z, 0.0f);
+                    f3v = make_float4(al.x, al.y, al.z, 0.0f);
+                }
+            } else if (st.skybox_color_texture_id >= 0) {
+                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+            }
+            add_glow(S, ray, hit_distance, current);
+            color = mul_add(current, throughput, color);
+            if (query) {
+                A.path_color[pixel] = make_float4(color.x, color.y, color.z, pc.w);
+            } else {
+                float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
+                set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, pc.w);
+            }
+        }
+        uint32_t q = warp_append(C.count, query);
+        if (query) {
+            float4 *f = C.features + 4 * (size_t)q;
+            f[0] = f0; f[1] = f1; f[2] = f2; f[3] = f3v;
+            C.aux[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __uint_as_float(pixel));
+            C.aux[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(cone_pixel));
+        }
+    }
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// Training paths: query j of the frame's training set restarts from the
+// query's ray with zero colour and unit throughput in its own slot j.  With
+// more queries than training paths the set is stratified: j takes query
+// floor((j + offset) * queries / capacity).
+__global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
+    const uint32_t nq = *C.count, cap = C.train_capacity;
+    const uint32_t n = nq < cap ? nq : cap;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        uint32_t idx = j;
+        if (nq > cap) {
+            idx = (uint32_t)(((double)j + (double)C.offset) * (double)nq / (double)cap);
+            if (idx >= nq) idx = nq - 1;
+        }
+        if (C.t_features) {
+            const float4 *f = C.features + 4 * (size_t)idx;
+            float4 *t = C.t_features + 4 * (size_t)j;
+            t[0] = f[0]; t[1] = f[1]; t[2] = f[2]; t[3] = f[3];
+        }
+        float4 a = C.aux[2 * (size_t)idx], b = C.aux[2 * (size_t)idx + 1];
+        rays[2 * (size_t)j] = make_float4(a.x, a.y, a.z, __uint_as_float(j));
+        rays[2 * (size_t)j + 1] = b;
+        C.t_color[j] = make_float4(0.0f, 0.0f, 0.0f, INFINITY);
+        C.t_through[j] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *C.train_count = n;
+        *ray_count = n;
+    }
+}
+
+// Waiting paths take the cache's answer: colour += throughput * radiance,
+// then tone mapping and the canvas write of k_shade.
+__global__ void k_cache_resolve(DevFrame F, CacheArgs C, const float4 *path_color, const float4 *path_throughput) {
+    const uint32_t nq = *C.count;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        uint32_t pixel = __float_as_uint(C.aux[2 * (size_t)q].w);
+        float4 pc = path_color[pixel];
+        float3 thr = xyz(path_throughput[pixel]);
+        float3 L = f3(0, 0, 0);
+        if (C.mode == SLIM_CACHE_ON) L = xyz(C.radiance[q]);
+        else if (C.mode == SLIM_CACHE_EXACT) L = xyz(C.t_targets[q]);
+        float3 color = mul_add(L, thr, xyz(pc));
+        float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
+        set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, pc.w);
+    }
+}
+
 template <bool COUNT>
 cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block, cudaStream_t stream,
-                      StageTimer *timer) {
+                      StageTimer *timer, const CacheFrame *cache) {
     uint32_t samples = F.width * F.height;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -536,39 +686,69 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     A.path_color = B.path_color;
     A.path_throughput = B.path_throughput;
     A.samples = samples;
-    uint32_t max_depth = F.settings.max_depth;
-    for (uint32_t depth = 1; depth <= max_depth; depth++) {
-        uint32_t in = (depth - 1) & 1, out = depth & 1;
+    const uint32_t max_depth = F.settings.max_depth;
+    const bool use_cache = cache && cache->mode != SLIM_CACHE_OFF && cache->depth >= 2 && cache->depth <= max_depth;
+    CacheArgs CA{};
+    if (use_cache) {
+        CA.features = cache->features;
+        CA.aux = cache->aux;
+        CA.radiance = cache->radiance;
+        CA.count = cache->counts;
+        CA.train_count = cache->counts + 1;
+        CA.train_capacity = cache->train_capacity;
+        CA.t_features = cache->mode == SLIM_CACHE_ON ? cache->t_features : nullptr;
+        CA.t_targets = cache->t_targets;
+        CA.t_color = cache->t_color;
+        CA.t_through = cache->t_through;
+        CA.offset = cache->select_offset;
+        CA.mode = cache->mode;
+        e = cudaMemsetAsync(cache->counts, 0, 2 * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return e;
+    }
+    const uint32_t bound = samples;   // a queue holds at most one ray per sample
+
+    // One bounce round over the queue `in` (primary rays at depth 1): extend,
+    // then shadows and shading -- or, at the cache depth, the cache gather.
+    uint32_t in = 0;
+    auto round = [&](uint32_t depth, bool primary, bool gather) -> cudaError_t {
+        uint32_t out = in ^ 1u;
         A.depth = depth;
-        A.rays_in = depth == 1 ? nullptr : B.rays[in];
-        A.count_in = depth == 1 ? nullptr : B.queue_count + in;
+        A.rays_in = primary ? nullptr : B.rays[in];
+        A.count_in = primary ? nullptr : B.queue_count + in;
         A.rays_out = B.rays[out];
         A.count_out = B.queue_count + out;
         // the output queue of this round is the input of the next: clear it
-        if (depth > 1) {
-            e = cudaMemsetAsync(B.queue_count + out, 0, sizeof(uint32_t), stream);
-            if (e != cudaSuccess) return e;
+        if (!primary) {
+            cudaError_t r = cudaMemsetAsync(B.queue_count + out, 0, sizeof(uint32_t), stream);
+            if (r != cudaSuccess) return r;
         }
-        uint32_t bound = depth == 1 ? samples : samples;   // queue length is at most one ray per sample
         A.counters = stage_counters(STAGE_EXTEND);
         if (timer) timer->begin(STAGE_EXTEND, stream);
         k_extend<COUNT><<<grid_for((const void *)k_extend<COUNT>, bound), block, 0, stream>>>(S, F, A);
         if (timer) timer->end(STAGE_EXTEND, stream);
+        if (gather) {
+            A.counters = stage_counters(STAGE_CACHE);
+            if (timer) timer->begin(STAGE_CACHE, stream);
+            k_cache_gather<COUNT><<<grid_for((const void *)k_cache_gather<COUNT>, bound), block, 0, stream>>>(S, F, A, CA);
+            if (timer) timer->end(STAGE_CACHE, stream);
+            in = out;
+            return cudaGetLastError();
+        }
         // Shadow rays in light batches that fit the shadow queue.
         uint32_t per_batch = B.shadow_capacity / (samples ? samples : 1);
         if (per_batch < 1) per_batch = 1;
         for (uint32_t l0 = 0; l0 < lights; l0 += per_batch) {
             A.light_begin = l0;
             A.light_end = l0 + per_batch < lights ? l0 + per_batch : lights;
-            e = cudaMemsetAsync(B.queue_count + 2, 0, sizeof(uint32_t), stream);
-            if (e != cudaSuccess) return e;
+            cudaError_t r = cudaMemsetAsync(B.queue_count + 2, 0, sizeof(uint32_t), stream);
+            if (r != cudaSuccess) return r;
             A.shadow_count = B.queue_count + 2;
             A.counters = stage_counters(STAGE_SHADOW_GEN);
             if (timer) timer->begin(STAGE_SHADOW_GEN, stream);
             k_shadow_gen<COUNT><<<grid_for((const void *)k_shadow_gen<COUNT>, bound), block, 0, stream>>>(S, F, A);
             if (timer) timer->end(STAGE_SHADOW_GEN, stream);
-            e = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
-            if (e != cudaSuccess) return e;
+            r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
+            if (r != cudaSuccess) return r;
             A.counters = stage_counters(STAGE_SHADOW);
             if (timer) timer->begin(STAGE_SHADOW, stream);
             k_shadow_scene<COUNT><<<grid_for((const void *)k_shadow_scene<COUNT>, bound * (A.light_end - A.light_begin)), block, 0, stream>>>(S, F, A);
@@ -582,21 +762,67 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
         if (timer) timer->begin(STAGE_SHADE, stream);
         k_shade<COUNT><<<grid_for((const void *)k_shade<COUNT>, bound), block, 0, stream>>>(S, F, A);
         if (timer) timer->end(STAGE_SHADE, stream);
-        e = cudaGetLastError();
+        in = out;
+        return cudaGetLastError();
+    };
+
+    const uint32_t last = use_cache ? cache->depth : max_depth;
+    for (uint32_t depth = 1; depth <= last; depth++)
+        if ((e = round(depth, depth == 1, use_cache && depth == last)) != cudaSuccess) return e;
+    if (!use_cache) return cudaSuccess;
+
+    const int mode = cache->mode;
+    const bool train = mode == SLIM_CACHE_ON && cache->trainer && cache->batch && cache->train_capacity;
+    if (mode == SLIM_CACHE_EXACT || train) {
+        // training paths continue from the cache vertex in their own slots
+        if (timer) timer->begin(STAGE_CACHE, stream);
+        uint32_t g = (cache->train_capacity + 255) / 256;
+        if (g > (uint32_t)(sms * 8)) g = (uint32_t)(sms * 8);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in);
+        if (timer) timer->end(STAGE_CACHE, stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        QueueArgs main = A;
+        A.path_color = cache->t_color;
+        A.path_throughput = cache->t_through;
+        A.sink = cache->t_targets;
+        A.skip_glow_depth = cache->depth;
+        for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
+            if ((e = round(depth, false, false)) != cudaSuccess) return e;
+        A = main;
+    }
+    if (train) {
+        if (timer) timer->begin(STAGE_CACHE_TRAIN, stream);
+        for (uint32_t off = 0; off < cache->train_capacity; off += cache->batch) {
+            uint32_t n = cache->train_capacity - off < cache->batch ? cache->train_capacity - off : cache->batch;
+            if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, stream)) !=
+                cudaSuccess)
+                return e;
+        }
+        if (timer) timer->end(STAGE_CACHE_TRAIN, stream);
+    }
+    if (mode == SLIM_CACHE_ON) {
+        if (timer) timer->begin(STAGE_CACHE_QUERY, stream);
+        e = nrc::launch_infer(cache->features, cache->counts, 0, samples, cache->radiance, cache->weights,
+                              F.error_flags, stream);
+        if (timer) timer->end(STAGE_CACHE_QUERY, stream);
         if (e != cudaSuccess) return e;
     }
-    return cudaSuccess;
+    if (timer) timer->begin(STAGE_CACHE, stream);
+    k_cache_resolve<<<grid_for((const void *)k_cache_resolve, bound), block, 0, stream>>>(F, CA, B.path_color,
+                                                                                          B.path_throughput);
+    if (timer) timer->end(STAGE_CACHE, stream);
+    return cudaGetLastError();
 }
 
 }  // namespace dev
 
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream, StageTimer *timer) {
+                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache) {
     if (F.settings.render_mode != SLIM_RENDER_BEAUTY)   // a single primary hit: nothing to queue
         return launch_render_fused(S, F, block, stream, timer);
     if (F.settings.max_depth == 0) return launch_render_fused(S, F, block, stream, timer);
-    if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer);
-    return dev::run_frame<false>(S, F, B, block, stream, timer);
+    if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer, cache);
+    return dev::run_frame<false>(S, F, B, block, stream, timer, cache);
 }
 
 }  // namespace slim

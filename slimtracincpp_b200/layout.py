@@ -89,7 +89,15 @@ SETTINGS = _dt([("max_depth", u1, 0), ("skybox_color_texture_id", i1, 1), ("skyb
                 ("skybox_irradiance_texture_id", i1, 3), ("render_mode", i4, 4), ("mip_level_colors", (i4, 9), 8)], 44)
 RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4, 8), ("block_size", i4, 12),
                       ("count_work", i4, 16), ("profile_stages", i4, 20), ("shadow_queue_mb", i4, 24),
-                      ("_reserved", i4, 28)], 32)
+                      ("radiance_cache", i4, 28)], 32)
+CACHE_CONFIG = _dt([("cache_depth", u4, 0), ("train_samples", u4, 4), ("batch", u4, 8), ("seed", u4, 12),
+                    ("learning_rate", f4, 16), ("beta1", f4, 20), ("beta2", f4, 24), ("epsilon", f4, 28),
+                    ("train", u4, 32), ("_reserved", (u4, 3), 36)], 48)
+CACHE_STATS = _dt([("frames", u8, 0), ("steps", u8, 8), ("queries", u4, 16), ("train_samples", u4, 20),
+                   ("loss", f4, 24), ("_pad", f4, 28)], 32)
+CACHE_OFF, CACHE_ON, CACHE_TRUNCATE, CACHE_EXACT = 0, 1, 2, 3
+NRC_PARAMS = 18624
+NRC_FEATURES = 16
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(
     ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",
      "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels"])], 80)

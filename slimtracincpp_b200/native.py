@@ -17,7 +17,7 @@ from . import layout as L
 LIB_PATH = Path(os.environ.get("SLIMTRACER_LIB", Path(__file__).resolve().parent / "_native" / "libslimtracer_b200.so"))
 
 SLIM_OK = 0
-ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "LIMIT", 5: "IO", 6: "STACK"}
+ERRORS = {1: "ARGUMENT", 2: "CUDA", 3: "STATE", 4: "LIMIT", 5: "IO", 6: "STACK", 7: "TIMEOUT"}
 
 EXPORTS = [
     "slimInitDataOnGPU", "slimUploadLights", "slimUploadCameras", "slimUploadGeometries", "slimUploadMaterials",
@@ -26,6 +26,9 @@ EXPORTS = [
     "slimProjectionReset", "slimBuildSceneBVH", "slimBuildMesh", "slimReadMeshHeader", "slimReadMesh",
     "slimWriteMesh", "slimReadTextureHeader", "slimReadTexture", "slimWriteTexture", "slimBakeTexture",
     "slimGetStageStats", "slimResetStageStats", "slimRenderToDeviceNoAlloc",
+    "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
+    "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
+    "slimRadianceCacheTrain", "slimRadianceCacheGetStats",
 ]
 
 
@@ -71,6 +74,12 @@ def lib():
     h.slimBakeTexture.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
     h.slimGetStageStats.argtypes = [P, C.c_int, P]
     h.slimResetStageStats.argtypes = []
+    for name in ["slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheGetStats"]:
+        getattr(h, name).argtypes = [P]
+    for name in ["slimRadianceCacheSetWeights", "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients"]:
+        getattr(h, name).argtypes = [P, C.c_uint32]
+    h.slimRadianceCacheQuery.argtypes = [P, C.c_uint32, P, P]
+    h.slimRadianceCacheTrain.argtypes = [P, P, C.c_uint32, P]
     for name in EXPORTS:
         if name not in ("slimGetLastError",):
             getattr(h, name).restype = C.c_int
@@ -104,11 +113,13 @@ def projection_reset(orientation9, position3, focal_length, width, height, ssaa=
 
 
 def set_render_options(engine=L.ENGINE_WAVEFRONT, ray_cones=L.CONES_REFERENCE, scene_bvh=L.SCENE_BVH_UPLOADED,
-                       block_size=0, count_work=False, profile_stages=False, shadow_queue_mb=0):
+                       block_size=0, count_work=False, profile_stages=False, shadow_queue_mb=0,
+                       radiance_cache=L.CACHE_OFF):
     o = np.zeros((), L.RENDER_OPTIONS)
     o["engine"], o["ray_cones"], o["scene_bvh"] = engine, ray_cones, scene_bvh
     o["block_size"], o["count_work"] = block_size, int(bool(count_work))
     o["profile_stages"], o["shadow_queue_mb"] = int(bool(profile_stages)), shadow_queue_mb
+    o["radiance_cache"] = radiance_cache
     check(lib().slimSetRenderOptions(ptr(o)))
 
 

@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
     p.add_argument("--seed", type=int, default=0)
-    p.add_argument("--config", default="config2", choices=["config1", "config2", "config3", "config4"],
+    p.add_argument("--config", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
                    help="workload (default: config2, the metric's 1080p mesh PBR scene)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
@@ -335,6 +335,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     for _ in range(args.warmup):
         native.check(lib.slimRefitSceneBVH(sp))
         r.render_to_device(vp, outs[0][0].data_ptr(), outs[0][1].data_ptr(), sp)
+    cache.join(sp)
     torch.cuda.synchronize()
     native.reset_stage_stats()
     clocks = ClockSampler(local, device_uuid(dev))
@@ -342,7 +343,18 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    cache_ms = timed_frames(torch, native, r, vp, sp, stream, outs, flush)
+    # Frames back to back; the cache trains each frame's paths on its second
+    # stream while the next frame runs, so the span from the first frame's
+    # start to the join of the last frame's training is the honest total.
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    launches0 = native.launch_count()
+    frame_ms = timed_frames(torch, native, r, vp, sp, stream, outs, flush)
+    launches = native.launch_count() - launches0
+    cache.join(sp)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    cache_ms = [t_start.elapsed_time(t_end) / steps] * steps
     if world > 1:
         dist.barrier()
     clock_info = clocks.stop()
@@ -414,6 +426,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
                              "stages_ms_per_frame": plain_stages},
             "speedup_vs_plain_depth8": plain_total / cache_total,
             "psnr_db_per_frame": psnr, "max_abs_per_frame": max_abs,
+            "frame_event_ms": frame_ms,
             "cache": {"queries": cstats["queries"], "train_samples": cstats["train_samples"],
                       "loss": cstats["loss"], "steps": cstats["steps"], "frames": cstats["frames"]},
             "stages_ms_per_frame": stages, "dominant_stage": dom,
@@ -423,12 +436,121 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
                     "d2h_bytes_per_step": int(pin_pix.numel() * 4 + pin_dep.numel() * 4),
                     "ms_per_step": 1000.0 * e2e_s / steps},
             "clocks": clock_info,
-            "gpu_launches": None}
-    # our kernels per cache frame: trace stages + cache stages (train = 2 kernels per step)
-    per_frame = 0
-    for k, v in stats.items():
-        per_frame += v["launches"] * (2 if k == "refit" else 8 if k == "cache_train" else 1)
-    line["gpu_launches"] = per_frame
+            "gpu_launches": launches}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_batch_bench(args, torch, dist, dev, rank, world, local):
+    """Config 5: 64 requests (own seeded scenes, 320x180 ... 3840x2160, depth
+    1-8, every other one with the radiance cache) rendered as one batch --
+    waves over shared queues, captured in a CUDA graph, plan chosen by the
+    project autotuner -- against rendering them one at a time (a batch of
+    one each, same kernels, same graph replay)."""
+    import numpy as np
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200 import native, scenes
+    from slimtracincpp_b200.batch import BatchRenderer
+    from slimtracincpp_b200.radiance_cache import RadianceCache
+    from slimtracincpp_b200.scene import Scene, geometry
+    meshes = scenes.config2_meshes()
+    reqs = scenes.config5(args.seed, meshes=meshes)
+    assets = Scene(np.array([geometry(L.GEOMETRY_SPHERE, 0)]), np.array([L.default_material()]), meshes=meshes)
+    batch = BatchRenderer(assets)
+    RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=args.seed)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    outs = [(torch.zeros((q.samples, 4), dtype=torch.float32, device=dev),
+             torch.zeros(q.samples, dtype=torch.float32, device=dev)) for q in reqs]
+    ptrs = [(p.data_ptr(), d.data_ptr()) for p, d in outs]
+    pixels = sum(q.samples for q in reqs)
+
+    # rays of one batch, counted by the kernels (untimed)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, count_work=True)
+    batch.set_requests(reqs, ptrs)
+    batch.render(sp)
+    batch.synchronize(sp)
+    wk = native.work_counters()
+    rays = wk["primary_rays"] + wk["shadow_rays"] + wk["bounce_rays"]
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+
+    batch.set_requests(reqs, ptrs)
+    plan = batch.tune(sp)
+    for _ in range(args.warmup):
+        batch.render(sp)
+    batch.synchronize(sp)
+    clocks = ClockSampler(local, device_uuid(dev))
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = native.launch_count()
+    for i in range(args.steps):
+        starts[i].record(stream)
+        batch.render(sp)
+        ends[i].record(stream)
+    launches = native.launch_count() - launches0
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    batch_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    plan = batch.plan()
+
+    # end to end: the batch plus every canvas read back to pinned host memory
+    pins = [(torch.empty_like(p, device="cpu").pin_memory(), torch.empty_like(d, device="cpu").pin_memory())
+            for p, d in outs]
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 4)):
+        batch.render(sp)
+        for (hp, hd), (p, d) in zip(pins, outs):
+            hp.copy_(p, non_blocking=True)
+            hd.copy_(d, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_steps = max(1, args.steps // 4)
+    e2e_s = time.perf_counter() - t0
+    d2h = sum(p.numel() * 4 + d.numel() * 4 for p, d in outs)
+
+    # one at a time: each request as a batch of one, same plan, graph replay
+    single_ms = []
+    for q, ptr in zip(reqs, ptrs):
+        batch.set_requests([q], [ptr])
+        batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"])
+        batch.render(sp)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(3):
+            batch.render(sp)
+        b.record(stream)
+        torch.cuda.synchronize()
+        single_ms.append(a.elapsed_time(b) / 3)
+
+    times = torch.tensor([sum(batch_ms), e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    total_ms, e2e_s = float(times[0]), float(times[1])
+    ms = total_ms / args.steps
+    value = rays * args.steps * world / (total_ms / 1000.0) / 1e6
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 trace, bf16 MLP (f32 accumulate)",
+            "data": "synthetic (64 seeded request scenes)",
+            "config": {"workload": "config5_batch_64_requests", "requests": len(reqs), "pixels": pixels,
+                       "rays_per_batch": rays, "cache_requests": sum(q.radiance_cache != 0 for q in reqs),
+                       "resolutions": [f"{q.width}x{q.height}" for q in reqs],
+                       "max_depths": [int(q.settings["max_depth"]) for q in reqs],
+                       "parallelism": f"replicas x{world}",
+                       "l2": "no flush: canvases and queues (> 3 GB) exceed L2"},
+            "batch_ms": ms, "plan": plan,
+            "one_at_a_time": {"total_ms": sum(single_ms), "per_request_ms": single_ms,
+                              "mrays_s": rays / (sum(single_ms) / 1000.0) / 1e6},
+            "speedup_vs_one_at_a_time": sum(single_ms) / ms,
+            "e2e": {"value": rays * e2e_steps * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000.0 * e2e_s / e2e_steps},
+            "clocks": clock_info,
+            "gpu_launches": launches}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -450,6 +572,8 @@ def main():
     torch.cuda.set_device(dev)
     if args.config == "config4":
         return run_cache_bench(args, torch, dist, dev, rank, world, local)
+    if args.config == "config5":
+        return run_batch_bench(args, torch, dist, dev, rank, world, local)
 
     from slimtracincpp_b200 import layout as L
     from slimtracincpp_b200 import native, scenes
@@ -501,12 +625,14 @@ def main():
     torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = native.launch_count()
     for i in range(args.steps):
         flush.zero_()
         starts[i].record(stream)
         native.check(lib.slimRefitSceneBVH(sp))
         r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
         ends[i].record(stream)
+    launches = native.launch_count() - launches0
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -566,8 +692,6 @@ def main():
                     "traffic": None, "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
                     "share_of_frame": d["total_ms"] / total_ms}
     frame_bytes = algorithmic_bytes(work)
-    # kernels of this library in the timed region (refit = leaves + inner kernels)
-    launches = sum(v["launches"] * (2 if k == "refit" else 1) for k, v in stats.items())
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -190,7 +190,7 @@ typedef struct {
                                 cone (mip 0: its copy of the aux hit clears the per-pixel
                                 spread); SLIM_CONES_PER_PIXEL: per-pixel spread */
     int32_t scene_bvh;       /* SLIM_SCENE_BVH_UPLOADED (default) or GPU refit of its topology */
-    int32_t block_size;      /* threads per block, 0 = tuned default */
+    int32_t block_size;      /* threads per block (multiple of 32, at most 256), 0 = tuned default */
     int32_t count_work;      /* non-zero: accumulate per-frame work counters (slower) */
     int32_t profile_stages;  /* non-zero: time every stage launch with CUDA events */
     int32_t shadow_queue_mb; /* wavefront shadow-ray queue budget in MiB, 0 = 1024 */
@@ -264,6 +264,15 @@ int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection 
 
 const char *slimGetLastError(void);
 int slimGetVersion(void);
+
+/* Waits for `stream` and reports what the device flagged since the last
+ * check (stack overflow, bad index, a timed-out wait) and, with
+ * options.count_work, the work counters of the last frame or batch. */
+int slimSynchronize(void *stream);
+
+/* Kernels this library has launched since it was loaded (a replayed batch
+ * graph counts its kernel nodes). */
+int slimGetLaunchCount(uint64_t *count);
 
 int slimSetRenderOptions(const SlimRenderOptions *options);
 int slimGetRenderOptions(SlimRenderOptions *options);
@@ -342,7 +351,11 @@ typedef struct {
     float learning_rate;     /* 1e-2 */
     float beta1, beta2, epsilon;   /* 0.9, 0.99, 1e-8 */
     uint32_t train;          /* non-zero: train online every rendered frame */
-    uint32_t _reserved[3];
+    uint32_t overlap;        /* non-zero: trace the training paths and take the Adam steps
+                                on a second stream, one frame behind: a frame's queries are
+                                answered with the weights trained through the previous frame,
+                                while its own training overlaps the next frame's rays */
+    uint32_t _reserved[2];
 } SlimRadianceCacheConfig;
 typedef struct {
     uint64_t frames, steps;  /* frames rendered with the cache, Adam steps taken */
@@ -367,7 +380,58 @@ int slimRadianceCacheGetGradients(float *grad, uint32_t count);
 int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radiance, void *stream);
 /* One Adam step over `count` (features, target float4 rgb) device samples. */
 int slimRadianceCacheTrain(const void *d_features, const void *d_targets, uint32_t count, void *stream);
+/* Makes `stream` wait for the cache's overlapped training (no-op without). */
+int slimRadianceCacheJoin(void *stream);
 int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats);
+
+/* ---- Batched requests.  No counterpart in the reference. ----------------
+ * Many render requests, each with its own scene, camera, settings and
+ * canvas, traced together: their pixels are cut into tiles, consecutive
+ * tiles fill waves of up to `queue_capacity` paths, and every wave runs the
+ * wavefront stage kernels once for all of its requests (each path looks up
+ * its request's scene and canvas).  The whole batch is captured into a CUDA
+ * graph on the first slimBatchRender and replayed afterwards.  Mesh and
+ * texture ids of every request refer to the assets uploaded by
+ * slimInitDataOnGPU (a request's scene->meshes / ->textures are not read). */
+typedef struct {
+    const SlimSceneData *scene;        /* geometries, materials, lights, scene BVH + leaf indices, flags */
+    SlimCameraRayProjection projection;
+    SlimRayTracerSettings settings;    /* beauty mode only */
+    uint32_t width, height;            /* canvas pixels (no SSAA in a batch) */
+    int32_t radiance_cache;            /* SLIM_CACHE_OFF or SLIM_CACHE_ON (needs a configured cache) */
+    uint32_t _pad;
+    void *d_pixels;                    /* device: float4 per pixel */
+    void *d_depths;                    /* device: float per pixel */
+} SlimRenderRequest;
+
+typedef struct {
+    uint32_t queue_capacity;   /* path slots per wave */
+    uint32_t tile_pixels;      /* pixels per tile (a tile never spans two waves) */
+    int32_t block_size;        /* threads per block of the stage kernels (32..256) */
+    uint32_t waves;            /* out: waves of the current requests */
+    float batch_ms;            /* out: one batch with this plan, when it was tuned */
+    uint32_t candidates;       /* out: plans the tuner timed */
+    uint32_t graph_nodes;      /* out: kernel nodes of the captured graph (0 before the first render) */
+    uint32_t tuned;            /* out: non-zero when slimBatchTune chose the plan */
+} SlimBatchPlan;
+
+/* Uploads the requests (validated like slimInitDataOnGPU) and drops any
+ * captured graph.  At most 512 requests of at most 2^23 pixels each. */
+int slimBatchSetRequests(const SlimRenderRequest *requests, uint32_t count);
+/* Project autotuner: times candidate plans (queue capacity, tile size, block
+ * size) on the current requests with CUDA events and keeps the fastest. */
+int slimBatchTune(void *stream);
+int slimBatchSetPlan(const SlimBatchPlan *plan);
+int slimBatchGetPlan(SlimBatchPlan *plan);
+/* Renders every request (asynchronous on `stream`): the first call after
+ * slimBatchSetRequests / slimBatchSetPlan captures the batch into a CUDA
+ * graph, later calls replay it. */
+int slimBatchRender(void *stream);
+
+SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheConfig) == 48, "RadianceCacheConfig is 48 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheStats) == 32, "RadianceCacheStats is 32 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimRenderRequest) == 184, "RenderRequest is 184 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimBatchPlan) == 32, "BatchPlan is 32 bytes");
 
 /* Host-side helpers: the reference's own host algorithms, restated. */
 

@@ -27,7 +27,7 @@ BUILD_DIR = ROOT / "_build" / "slimtracer"
 
 CUDA_SOURCES = ["api.cu", "kernels_fused.cu", "kernels_wavefront.cu", "kernels_refit.cu", "kernels_nrc.cu"]
 HOST_SOURCES = ["host_assets.cpp", "texture_baker.cpp"]
-HEADERS = ["device_scene.h", "host_common.h", "kernels.h", "tracer_core.cuh"]
+HEADERS = ["device_scene.h", "host_common.h", "kernels.h", "tracer_core.cuh", "nrc.h", "umma.cuh", "launch_count.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--prec-div=true", "--prec-sqrt=true",

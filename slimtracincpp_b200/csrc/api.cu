@@ -2,6 +2,7 @@
 // plus the device-resident extensions.  One process-wide render context,
 // like the reference's module-global GPU mirror (renderer/renderer_GPU.h:
 // 12-20); calls are serialised by a mutex.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +19,8 @@
 #include "nrc.h"
 
 namespace slim {
+
+std::atomic<unsigned long long> g_kernel_launches{0};
 
 namespace {
 thread_local std::string g_error;
@@ -42,7 +45,12 @@ struct DevArray {
     size_t count = 0;
     int reserve(size_t n, const char *what) {
         if (n <= count && ptr) return SLIM_OK;
-        if (ptr) cudaFree(ptr);
+        // work in flight (the cache's overlapped training stream among it) may
+        // still read the old array
+        if (ptr) {
+            cudaDeviceSynchronize();
+            cudaFree(ptr);
+        }
         ptr = nullptr;
         count = 0;
         if (!n) return SLIM_OK;
@@ -95,18 +103,24 @@ struct Context {
         DevArray<uint8_t> image;
         DevArray<float4> features, aux, radiance, t_features, t_targets, t_color, t_through;
         DevArray<uint32_t> counts;
+        DevArray<uint32_t> state;      // [0] Adam steps taken, [1] cache frames (training-set offsets)
         uint32_t *error_flags = nullptr;
-        uint64_t steps = 0, frames = 0;
+        // overlapped training: second stream, its own queues, the queries' weight snapshot
+        cudaStream_t stream_b = nullptr;
+        cudaEvent_t ev_selected = nullptr, ev_trained = nullptr;
+        DevArray<uint8_t> image_infer;
+        DevArray<float4> tq_rays0, tq_rays1, tq_hits, tq_shadow, tq_pairs;
+        DevArray<uint32_t> tq_counts;
+        DevArray<unsigned long long> tq_masks;
+        WavefrontBuffers tq{};
         cudaError_t step(const float4 *f, const float4 *t, uint32_t samples, const uint32_t *count, uint32_t offset,
                          cudaStream_t stream) override {
-            steps++;
             nrc::AdamArgs a{};
             a.lr = config.learning_rate;
             a.beta1 = config.beta1;
             a.beta2 = config.beta2;
             a.eps = config.epsilon;
-            a.bias1 = (float)(1.0 / (1.0 - std::pow((double)config.beta1, (double)steps)));
-            a.bias2 = (float)(1.0 / (1.0 - std::pow((double)config.beta2, (double)steps)));
+            a.step = state.ptr;
             return nrc::launch_train_step(f, t, samples, count, offset, params.ptr, m.ptr, v.ptr, image.ptr,
                                           partials.ptr, loss_partials.ptr, grad.ptr, loss.ptr, a, error_flags, stream);
         }
@@ -531,17 +545,55 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     cf.t_targets = k.t_targets.ptr;
     cf.t_color = k.t_color.ptr;
     cf.t_through = k.t_through.ptr;
-    // stratified selection offset of this frame (SplitMix64 of seed and frame)
-    uint64_t z = ((uint64_t)k.config.seed << 32) + k.frames + 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    z ^= z >> 31;
-    cf.select_offset = (float)((z >> 40) * (1.0 / 16777216.0));
+    cf.frame_counter = k.state.ptr + 1;
     cf.batch = k.config.batch;
     cf.weights = k.image.ptr;
     cf.trainer = (mode == SLIM_CACHE_ON && k.config.train) ? &k : nullptr;
     k.error_flags = c.d_error.ptr;
-    k.frames++;
+    // Overlapped training (not while counting work: the counters of a frame
+    // must be complete when the frame's stream is).
+    if (cf.trainer && k.config.overlap && !c.options.count_work && cap) {
+        if (!k.stream_b) {
+            // highest priority: the training rounds are long chains of small
+            // launches that should take SMs as soon as the frame's blocks free them
+            int least = 0, greatest = 0;
+            cudaDeviceGetStreamPriorityRange(&least, &greatest);
+            SLIM_CUDA(cudaStreamCreateWithPriority(&k.stream_b, cudaStreamNonBlocking, greatest), "cache training stream");
+            SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_selected, cudaEventDisableTiming), "cache event");
+            SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_trained, cudaEventDisableTiming), "cache event");
+        }
+        size_t lights = c.scene.light_count ? c.scene.light_count : 1;
+        size_t instances = 0;
+        for (const SlimGeometry &g : c.geometries) instances += g.type == SLIM_GEOMETRY_MESH;
+        size_t shadow = (size_t)cap * lights, pairs = shadow * (instances < 4 ? (instances ? instances : 1) : 4);
+        if ((rc = k.tq_rays0.reserve(2 * (size_t)cap, "alloc training queues"))) return rc;
+        if ((rc = k.tq_rays1.reserve(2 * (size_t)cap, "alloc training queues"))) return rc;
+        if ((rc = k.tq_hits.reserve(3 * (size_t)cap, "alloc training queues"))) return rc;
+        if ((rc = k.tq_shadow.reserve(2 * shadow, "alloc training queues"))) return rc;
+        if ((rc = k.tq_pairs.reserve(3 * pairs, "alloc training queues"))) return rc;
+        if ((rc = k.tq_counts.reserve(8, "alloc training queues"))) return rc;
+        if ((rc = k.tq_masks.reserve(cap, "alloc training queues"))) return rc;
+        if ((rc = k.image_infer.reserve(nrc::kImgBytes, "alloc weight snapshot"))) return rc;
+        WavefrontBuffers &T = k.tq;
+        T.path_color = k.t_color.ptr;
+        T.path_throughput = k.t_through.ptr;
+        T.rays[0] = k.tq_rays0.ptr;
+        T.rays[1] = k.tq_rays1.ptr;
+        T.queue_count = k.tq_counts.ptr;
+        T.hits = k.tq_hits.ptr;
+        T.shadow_rays = k.tq_shadow.ptr;
+        T.shadow_mask = k.tq_masks.ptr;
+        T.pairs = k.tq_pairs.ptr;
+        T.capacity = cap;
+        T.shadow_capacity = (uint32_t)shadow;
+        T.pair_capacity = (uint32_t)pairs;
+        cf.train_stream = k.stream_b;
+        cf.selected = k.ev_selected;
+        cf.trained = k.ev_trained;
+        cf.train_queues = &k.tq;
+        cf.train_weights = k.image.ptr;
+        cf.weights = k.image_infer.ptr;
+    }
     return SLIM_OK;
 }
 
@@ -680,6 +732,10 @@ int read_counters(Context &c, cudaStream_t stream) {
 
 using namespace slim;
 
+// A batch's tables point into the shared mesh and texture arrays and its
+// graph into the cache's weights: re-initialising either drops the batch.
+static void invalidate_batch();
+
 extern "C" {
 
 int slimGetVersion(void) { return 1; }
@@ -690,6 +746,7 @@ int slimInitDataOnGPU(const SlimSceneData *scene) {
     Context &c = g_ctx;
     int rc = ensure_device(c);
     if (rc) return rc;
+    invalidate_batch();
     if ((rc = check_scene_arrays(scene))) return rc;
     c.initialized = false;
     c.counts = scene->counts;
@@ -806,11 +863,28 @@ int slimTracePrimary(const SlimCameraRayProjection *projection, int width, int h
     return read_errors(c, (cudaStream_t)stream);
 }
 
+int slimGetLaunchCount(uint64_t *count) {
+    if (!count) return set_error(SLIM_ERR_ARGUMENT, "count is null");
+    *count = g_kernel_launches.load();
+    return SLIM_OK;
+}
+
+int slimSynchronize(void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (c.cache.ev_trained) SLIM_CUDA(cudaStreamWaitEvent((cudaStream_t)stream, c.cache.ev_trained, 0), "join training");
+    SLIM_CUDA(cudaStreamSynchronize((cudaStream_t)stream), "synchronize");
+    int rc = read_errors(c, (cudaStream_t)stream);
+    if (rc) return rc;
+    return read_counters(c, (cudaStream_t)stream);
+}
+
 int slimSetRenderOptions(const SlimRenderOptions *options) {
     std::lock_guard<std::mutex> lock(g_mutex);
     if (!options) return set_error(SLIM_ERR_ARGUMENT, "options is null");
     if (options->engine < 0 || options->engine > 1 || options->ray_cones < 0 || options->ray_cones > 1 ||
-        options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 1024 ||
+        options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 256 ||
         (options->block_size % 32) || options->radiance_cache < SLIM_CACHE_OFF ||
         options->radiance_cache > SLIM_CACHE_EXACT)
         return set_error(SLIM_ERR_ARGUMENT, "bad render options");
@@ -1049,13 +1123,14 @@ int cache_sync_errors(Context &c) {
 
 int upload_cache_weights(Context &c, const float *params) {
     Context::Cache &k = c.cache;
+    SLIM_CUDA(cudaDeviceSynchronize(), "wait for cache training");
     SLIM_CUDA(cudaMemcpy(k.params.ptr, params, nrc::kParams * sizeof(float), cudaMemcpyHostToDevice), "upload weights");
     SLIM_CUDA(cudaMemset(k.m.ptr, 0, nrc::kParams * sizeof(float)), "clear adam");
     SLIM_CUDA(cudaMemset(k.v.ptr, 0, nrc::kParams * sizeof(float)), "clear adam");
     SLIM_CUDA(cudaMemset(k.grad.ptr, 0, nrc::kParams * sizeof(float)), "clear gradient");
     SLIM_CUDA(cudaMemset(k.loss.ptr, 0, sizeof(float)), "clear loss");
     SLIM_CUDA(nrc::launch_pack_weights(k.params.ptr, k.image.ptr, nullptr), "pack weights");
-    k.steps = 0;
+    SLIM_CUDA(cudaMemset(k.state.ptr, 0, sizeof(uint32_t)), "clear step count");
     return cache_sync_errors(c);
 }
 
@@ -1074,6 +1149,8 @@ int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
         k.train_samples > (1u << 26))
         return set_error(SLIM_ERR_ARGUMENT, "bad radiance cache config");
     Context::Cache &st = c.cache;
+    invalidate_batch();
+    SLIM_CUDA(cudaDeviceSynchronize(), "wait for cache training");
     int rc;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
@@ -1085,9 +1162,11 @@ int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
     if ((rc = st.loss_partials.reserve((size_t)sms, "alloc partial losses"))) return rc;
     if ((rc = st.loss.reserve(1, "alloc loss"))) return rc;
     if ((rc = st.image.reserve(nrc::kImgBytes, "alloc weight image"))) return rc;
+    if ((rc = st.state.reserve(2, "alloc cache counters"))) return rc;
+    SLIM_CUDA(cudaMemset(st.state.ptr, 0, 2 * sizeof(uint32_t)), "clear cache counters");
     st.config = k;
-    st.frames = 0;
     st.error_flags = c.d_error.ptr;
+    SLIM_CUDA(nrc::prepare(), "radiance cache kernel attributes");
     std::vector<float> w;
     init_cache_weights(k.seed, w);
     if ((rc = upload_cache_weights(c, w.data()))) return rc;
@@ -1138,6 +1217,7 @@ int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radia
     Context &c = g_ctx;
     if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
     if ((!d_features || !d_radiance) && count) return set_error(SLIM_ERR_ARGUMENT, "null device buffer");
+    if (c.cache.ev_trained) SLIM_CUDA(cudaStreamWaitEvent((cudaStream_t)stream, c.cache.ev_trained, 0), "join training");
     cudaError_t e = nrc::launch_infer((const float4 *)d_features, nullptr, count, count, (float4 *)d_radiance,
                                       c.cache.image.ptr, c.d_error.ptr, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "cache query launch");
@@ -1157,6 +1237,13 @@ int slimRadianceCacheTrain(const void *d_features, const void *d_targets, uint32
     return SLIM_OK;
 }
 
+int slimRadianceCacheJoin(void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (c.cache.ev_trained) SLIM_CUDA(cudaStreamWaitEvent((cudaStream_t)stream, c.cache.ev_trained, 0), "join training");
+    return SLIM_OK;
+}
+
 int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats) {
     std::lock_guard<std::mutex> lock(g_mutex);
     Context &c = g_ctx;
@@ -1165,8 +1252,10 @@ int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats) {
     int rc = cache_sync_errors(c);
     if (rc) return rc;
     memset(stats, 0, sizeof(*stats));
-    stats->frames = c.cache.frames;
-    stats->steps = c.cache.steps;
+    uint32_t state[2] = {0, 0};
+    SLIM_CUDA(cudaMemcpy(state, c.cache.state.ptr, sizeof(state), cudaMemcpyDeviceToHost), "read cache counters");
+    stats->steps = state[0];
+    stats->frames = state[1];
     SLIM_CUDA(cudaMemcpy(&stats->loss, c.cache.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost), "read loss");
     if (c.cache.counts.ptr) {
         uint32_t counts[2] = {0, 0};
@@ -1174,6 +1263,487 @@ int slimRadianceCacheGetStats(SlimRadianceCacheStats *stats) {
         stats->queries = counts[0];
         stats->train_samples = counts[1];
     }
+    return SLIM_OK;
+}
+
+}  // extern "C"
+
+// ---- batched requests -------------------------------------------------------
+namespace {
+
+struct BatchState {
+    std::vector<SlimRenderRequest> requests;
+    std::vector<DevScene> h_scenes;
+    std::vector<DevFrame> h_frames;
+    DevArray<float4> geometries, scene_nodes;
+    DevArray<SlimMaterial> materials;
+    DevArray<SlimLight> lights;
+    DevArray<uint32_t> leaf_geometry, emissive;
+    DevArray<DevScene> scenes;
+    DevArray<DevFrame> frames;
+    DevArray<uint4> tiles;
+    std::vector<uint4> h_tiles;
+    std::vector<BatchWave> waves;
+    uint64_t pixels = 0;
+    uint32_t max_lights = 0, max_instances = 0;
+    bool any_cache = false;
+    SlimBatchPlan plan{};
+    // queues of a wave
+    DevArray<float4> color, through, rays0, rays1, hits, shadow_rays, pairs;
+    DevArray<uint32_t> counts;
+    DevArray<unsigned long long> masks;
+    WavefrontBuffers B{};
+    // cache queries of a wave (the batch's own buffers, so single frames never
+    // move what a captured batch graph points at)
+    CacheFrame cache{};
+    DevArray<float4> c_features, c_aux, c_radiance, c_targets, c_color, c_through, c_tfeatures;
+    DevArray<uint32_t> c_counts;
+    // captured batch
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_valid = false;
+    size_t graph_nodes = 0;
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        graph_valid = false;
+        graph_nodes = 0;
+    }
+};
+BatchState g_batch;
+
+}  // namespace
+
+static void invalidate_batch() {
+    g_batch.drop_graph();
+    g_batch.requests.clear();
+}
+
+namespace {
+
+constexpr uint32_t kBatchPixelBits = 23;
+
+// Pixels of every request cut into tiles; consecutive tiles fill waves of at
+// most queue_capacity slots.
+int plan_waves(BatchState &b) {
+    uint32_t Q = b.plan.queue_capacity, T = b.plan.tile_pixels;
+    if (T > Q) T = Q;
+    b.h_tiles.clear();
+    b.waves.clear();
+    BatchWave cur{};
+    uint32_t slot = 0;
+    auto close = [&]() {
+        if (cur.tile_count) b.waves.push_back(cur);
+        cur = BatchWave{};
+        cur.first_tile = (uint32_t)b.h_tiles.size();
+        slot = 0;
+    };
+    close();
+    for (uint32_t r = 0; r < b.requests.size(); r++) {
+        const SlimRenderRequest &q = b.requests[r];
+        const uint32_t n = q.width * q.height;
+        for (uint32_t first = 0; first < n; first += T) {
+            uint32_t count = n - first < T ? n - first : T;
+            if (slot + count > Q) close();
+            b.h_tiles.push_back(make_uint4(r, first, count, slot));
+            cur.tile_count++;
+            slot += count;
+            cur.samples = slot;
+            const DevFrame &f = b.h_frames[r];
+            if (f.settings.max_depth > cur.max_depth) cur.max_depth = f.settings.max_depth;
+            if (b.h_scenes[r].light_count > cur.max_lights) cur.max_lights = b.h_scenes[r].light_count;
+            if (f.cache_depth) cur.cache_paths = 1;
+        }
+    }
+    close();
+    int rc = b.tiles.reserve(b.h_tiles.size() ? b.h_tiles.size() : 1, "alloc batch tiles");
+    if (rc) return rc;
+    if (!b.h_tiles.empty())
+        SLIM_CUDA(cudaMemcpy(b.tiles.ptr, b.h_tiles.data(), b.h_tiles.size() * sizeof(uint4), cudaMemcpyHostToDevice),
+                  "upload batch tiles");
+    b.plan.waves = (uint32_t)b.waves.size();
+    return SLIM_OK;
+}
+
+// Queues for waves of queue_capacity paths (same sizing rule as a frame's).
+int ensure_batch_queues(BatchState &b) {
+    size_t Q = b.plan.queue_capacity;
+    size_t lights = b.max_lights ? b.max_lights : 1;
+    size_t budget = (size_t)1024 << 20;
+    size_t shadow = Q * lights, max_shadow = budget / (2 * sizeof(float4));
+    if (shadow > max_shadow) shadow = max_shadow < Q ? Q : max_shadow;
+    size_t inst = b.max_instances ? (b.max_instances < 4 ? b.max_instances : 4) : 1;
+    size_t pairs = shadow * inst, max_pairs = budget / (3 * sizeof(float4));
+    if (pairs > max_pairs) pairs = max_pairs;
+    int rc;
+    if ((rc = b.color.reserve(Q, "alloc batch paths"))) return rc;
+    if ((rc = b.through.reserve(Q, "alloc batch paths"))) return rc;
+    if ((rc = b.rays0.reserve(2 * Q, "alloc batch rays"))) return rc;
+    if ((rc = b.rays1.reserve(2 * Q, "alloc batch rays"))) return rc;
+    if ((rc = b.hits.reserve(3 * Q, "alloc batch hits"))) return rc;
+    if ((rc = b.shadow_rays.reserve(2 * shadow, "alloc batch shadow rays"))) return rc;
+    if ((rc = b.pairs.reserve(3 * pairs, "alloc batch shadow pairs"))) return rc;
+    if ((rc = b.counts.reserve(8, "alloc batch counters"))) return rc;
+    if ((rc = b.masks.reserve(Q, "alloc batch masks"))) return rc;
+    WavefrontBuffers &B = b.B;
+    B.path_color = b.color.ptr;
+    B.path_throughput = b.through.ptr;
+    B.rays[0] = b.rays0.ptr;
+    B.rays[1] = b.rays1.ptr;
+    B.queue_count = b.counts.ptr;
+    B.hits = b.hits.ptr;
+    B.shadow_rays = b.shadow_rays.ptr;
+    B.shadow_mask = b.masks.ptr;
+    B.pairs = b.pairs.ptr;
+    B.capacity = (uint32_t)Q;
+    B.shadow_capacity = (uint32_t)shadow;
+    B.pair_capacity = (uint32_t)pairs;
+    return SLIM_OK;
+}
+
+int batch_cache_frame(Context &c, BatchState &b) {
+    if (!b.any_cache) return SLIM_OK;
+    Context::Cache &k = c.cache;
+    if (!k.configured) return set_error(SLIM_ERR_STATE, "a request uses the radiance cache but it is not configured");
+    const uint32_t Q = b.plan.queue_capacity, cap = k.config.train_samples;
+    int rc;
+    if ((rc = b.c_features.reserve(4 * (size_t)Q, "alloc cache queries"))) return rc;
+    if ((rc = b.c_aux.reserve(2 * (size_t)Q, "alloc cache query rays"))) return rc;
+    if ((rc = b.c_radiance.reserve(Q, "alloc cache answers"))) return rc;
+    if ((rc = b.c_counts.reserve(2, "alloc cache counters"))) return rc;
+    if (cap) {
+        if ((rc = b.c_targets.reserve(cap, "alloc training targets"))) return rc;
+        if ((rc = b.c_color.reserve(cap, "alloc training paths"))) return rc;
+        if ((rc = b.c_through.reserve(cap, "alloc training paths"))) return rc;
+        if ((rc = b.c_tfeatures.reserve(4 * (size_t)cap, "alloc training samples"))) return rc;
+    }
+    CacheFrame &cf = b.cache;
+    cf = CacheFrame{};
+    cf.mode = SLIM_CACHE_ON;
+    cf.depth = k.config.cache_depth;
+    cf.features = b.c_features.ptr;
+    cf.aux = b.c_aux.ptr;
+    cf.radiance = b.c_radiance.ptr;
+    cf.counts = b.c_counts.ptr;
+    cf.train_capacity = cap;
+    cf.t_features = b.c_tfeatures.ptr;
+    cf.t_targets = b.c_targets.ptr;
+    cf.t_color = b.c_color.ptr;
+    cf.t_through = b.c_through.ptr;
+    cf.frame_counter = k.state.ptr + 1;
+    cf.batch = k.config.batch;
+    cf.weights = k.image.ptr;
+    cf.trainer = k.config.train ? &k : nullptr;
+    k.error_flags = c.d_error.ptr;
+    return SLIM_OK;
+}
+
+int batch_launch(Context &c, BatchState &b, cudaStream_t stream) {
+    BatchFrame BF{};
+    BF.shared = c.scene;
+    memset(&BF.frame, 0, sizeof(BF.frame));
+    BF.frame.error_flags = c.d_error.ptr;
+    BF.frame.counters = c.options.count_work ? c.d_counters.ptr : nullptr;
+    if (BF.frame.counters)
+        SLIM_CUDA(cudaMemsetAsync(BF.frame.counters, 0, kCountersPerStage * STAGE_COUNT * sizeof(unsigned long long), stream),
+                  "clear counters");
+    BF.scenes = b.scenes.ptr;
+    BF.frames = b.frames.ptr;
+    BF.tiles = b.tiles.ptr;
+    BF.waves = b.waves.data();
+    BF.wave_count = (uint32_t)b.waves.size();
+    BF.cache = b.any_cache ? &b.cache : nullptr;
+    cudaError_t e = launch_render_batch(BF, b.B, b.plan.block_size, stream, nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    return SLIM_OK;
+}
+
+// (Re)plans waves and queues for the current plan.
+int batch_prepare(Context &c, BatchState &b) {
+    int rc;
+    if ((rc = plan_waves(b))) return rc;
+    if ((rc = ensure_batch_queues(b))) return rc;
+    return batch_cache_frame(c, b);
+}
+
+int batch_time(Context &c, BatchState &b, cudaStream_t stream, int reps, float &ms) {
+    int rc = batch_prepare(c, b);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if ((rc = batch_launch(c, b, stream))) return rc;     // warm-up
+    cudaEventRecord(e0, stream);
+    for (int i = 0; i < reps && !rc; i++) rc = batch_launch(c, b, stream);
+    cudaEventRecord(e1, stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= (float)(reps > 0 ? reps : 1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "batch tuning");
+    return read_errors(c, stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int slimBatchSetRequests(const SlimRenderRequest *requests, uint32_t count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    BatchState &b = g_batch;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called (it uploads the shared assets)");
+    if (!requests || !count) return set_error(SLIM_ERR_ARGUMENT, "no requests");
+    if (count > (1u << (32 - kBatchPixelBits))) return set_error(SLIM_ERR_LIMIT, "more than 512 requests");
+    b.drop_graph();
+    b.requests.assign(requests, requests + count);
+    b.h_scenes.assign(count, DevScene{});
+    b.h_frames.assign(count, DevFrame{});
+    b.pixels = 0;
+    b.max_lights = b.max_instances = 0;
+    b.any_cache = false;
+    // validate and size the pools
+    size_t n_geo = 0, n_mat = 0, n_light = 0, n_node = 0;
+    for (uint32_t r = 0; r < count; r++) {
+        const SlimRenderRequest &q = requests[r];
+        const SlimSceneData *s = q.scene;
+        int rc = check_scene_arrays(s);
+        if (rc) return rc;
+        if (!q.width || !q.height || (uint64_t)q.width * q.height > (1ull << kBatchPixelBits))
+            return set_error(SLIM_ERR_LIMIT, "request canvas empty or above 2^23 pixels");
+        if (!q.d_pixels || !q.d_depths) return set_error(SLIM_ERR_ARGUMENT, "request without device canvas");
+        if (q.settings.render_mode != SLIM_RENDER_BEAUTY) return set_error(SLIM_ERR_ARGUMENT, "batched requests render beauty mode only");
+        if (q.radiance_cache != SLIM_CACHE_OFF && q.radiance_cache != SLIM_CACHE_ON)
+            return set_error(SLIM_ERR_ARGUMENT, "request radiance_cache must be OFF or ON");
+        for (uint32_t g = 0; g < s->counts.geometries; g++)
+            if (s->geometries[g].type == SLIM_GEOMETRY_MESH && s->geometries[g].id >= c.counts.meshes)
+                return set_error(SLIM_ERR_ARGUMENT, "request geometry names a mesh the shared assets lack");
+        for (uint32_t m = 0; m < s->counts.materials; m++) {
+            const SlimMaterial &mat = s->materials[m];
+            for (uint32_t k = 0; k < mat.texture_count && k < 2; k++)
+                if (mat.texture_ids[k] >= c.counts.textures && (mat.flags & (SLIM_MATERIAL_HAS_ALBEDO_MAP | SLIM_MATERIAL_HAS_NORMAL_MAP)))
+                    return set_error(SLIM_ERR_ARGUMENT, "request material names a texture the shared assets lack");
+        }
+        int8_t ids[3] = {q.settings.skybox_color_texture_id, q.settings.skybox_radiance_texture_id,
+                         q.settings.skybox_irradiance_texture_id};
+        for (int8_t id : ids)
+            if (id >= 0 && (uint32_t)id >= c.counts.textures) return set_error(SLIM_ERR_ARGUMENT, "request skybox texture id out of range");
+        if ((rc = check_bvh(s->bvh.nodes, s->bvh.node_count, s->counts.geometries, 0, "request scene BVH malformed"))) return rc;
+        if (!s->bvh_leaf_geometry_indices) return set_error(SLIM_ERR_ARGUMENT, "request scene BVH leaf indices missing");
+        if (bvh_depth(s->bvh.nodes, s->bvh.node_count) + 2 > (uint32_t)kStackCapacity)
+            return set_error(SLIM_ERR_LIMIT, "request scene BVH deeper than the traversal stack");
+        for (uint32_t g = 0; g < s->counts.geometries; g++)
+            if (s->bvh_leaf_geometry_indices[g] >= s->counts.geometries) return set_error(SLIM_ERR_ARGUMENT, "request BVH leaf index out of range");
+        n_geo += s->counts.geometries;
+        n_mat += s->counts.materials;
+        n_light += s->counts.lights;
+        n_node += s->bvh.node_count;
+    }
+    int rc;
+    if ((rc = b.geometries.reserve(4 * n_geo, "alloc batch geometries"))) return rc;
+    if ((rc = b.materials.reserve(n_mat, "alloc batch materials"))) return rc;
+    if ((rc = b.lights.reserve(n_light ? n_light : 1, "alloc batch lights"))) return rc;
+    if ((rc = b.scene_nodes.reserve(2 * n_node, "alloc batch scene BVHs"))) return rc;
+    if ((rc = b.leaf_geometry.reserve(n_geo, "alloc batch leaf indices"))) return rc;
+    if ((rc = b.emissive.reserve(n_geo, "alloc batch emissive lists"))) return rc;
+    if ((rc = b.scenes.reserve(count, "alloc batch scene table"))) return rc;
+    if ((rc = b.frames.reserve(count, "alloc batch frame table"))) return rc;
+    std::vector<float4> geo(4 * n_geo);
+    std::vector<SlimMaterial> mat;
+    std::vector<SlimLight> lig;
+    std::vector<SlimBVHNode> nodes;
+    std::vector<uint32_t> leaf, emis;
+    mat.reserve(n_mat);
+    lig.reserve(n_light);
+    nodes.reserve(n_node);
+    leaf.reserve(n_geo);
+    emis.reserve(n_geo);
+    size_t og = 0;
+    const uint32_t cache_depth = c.cache.configured ? c.cache.config.cache_depth : 0;
+    for (uint32_t r = 0; r < count; r++) {
+        const SlimRenderRequest &q = requests[r];
+        const SlimSceneData *s = q.scene;
+        DevScene S = c.scene;                  // shared mesh and texture arrays
+        S.geometries = b.geometries.ptr + 4 * og;
+        S.materials = b.materials.ptr + mat.size();
+        S.lights = b.lights.ptr + lig.size();
+        S.scene_nodes = b.scene_nodes.ptr + 2 * nodes.size();
+        S.leaf_geometry = b.leaf_geometry.ptr + leaf.size();
+        S.emissive_quads = b.emissive.ptr + emis.size();
+        S.geometry_count = s->counts.geometries;
+        S.material_count = s->counts.materials;
+        S.light_count = s->counts.lights;
+        S.scene_node_count = s->bvh.node_count;
+        S.flags = s->flags;
+        uint32_t emissive = 0, instances = 0;
+        for (uint32_t g = 0; g < s->counts.geometries; g++) {
+            const SlimGeometry &G = s->geometries[g];
+            pack_geometry(G, &geo[4 * (og + g)]);
+            if (G.type == SLIM_GEOMETRY_QUAD && (s->materials[G.material_id].flags & SLIM_MATERIAL_IS_EMISSIVE)) {
+                emis.push_back(g);
+                emissive++;
+            }
+            instances += G.type == SLIM_GEOMETRY_MESH;
+        }
+        S.emissive_quad_count = emissive;
+        og += s->counts.geometries;
+        mat.insert(mat.end(), s->materials, s->materials + s->counts.materials);
+        if (s->counts.lights) lig.insert(lig.end(), s->lights, s->lights + s->counts.lights);
+        nodes.insert(nodes.end(), s->bvh.nodes, s->bvh.nodes + s->bvh.node_count);
+        leaf.insert(leaf.end(), s->bvh_leaf_geometry_indices, s->bvh_leaf_geometry_indices + s->counts.geometries);
+        b.h_scenes[r] = S;
+        DevFrame F;
+        memset(&F, 0, sizeof(F));
+        F.projection = q.projection;
+        F.settings = q.settings;
+        F.width = q.width;
+        F.height = q.height;
+        F.stride = q.width;
+        F.antialias = SLIM_AA_NONE;
+        F.cones_per_pixel = c.options.ray_cones == SLIM_CONES_PER_PIXEL;
+        F.pixels = (float4 *)q.d_pixels;
+        F.depths = (float *)q.d_depths;
+        F.error_flags = c.d_error.ptr;
+        F.cache_depth = (q.radiance_cache == SLIM_CACHE_ON && cache_depth && q.settings.max_depth >= cache_depth) ? cache_depth : 0;
+        b.h_frames[r] = F;
+        b.pixels += (uint64_t)q.width * q.height;
+        if (s->counts.lights > b.max_lights) b.max_lights = s->counts.lights;
+        if (instances > b.max_instances) b.max_instances = instances;
+        b.any_cache |= F.cache_depth != 0;
+    }
+    SLIM_CUDA(cudaMemcpy(b.geometries.ptr, geo.data(), geo.size() * sizeof(float4), cudaMemcpyHostToDevice), "upload batch geometries");
+    SLIM_CUDA(cudaMemcpy(b.materials.ptr, mat.data(), mat.size() * sizeof(SlimMaterial), cudaMemcpyHostToDevice), "upload batch materials");
+    if (!lig.empty())
+        SLIM_CUDA(cudaMemcpy(b.lights.ptr, lig.data(), lig.size() * sizeof(SlimLight), cudaMemcpyHostToDevice), "upload batch lights");
+    SLIM_CUDA(cudaMemcpy(b.scene_nodes.ptr, nodes.data(), nodes.size() * sizeof(SlimBVHNode), cudaMemcpyHostToDevice), "upload batch BVHs");
+    SLIM_CUDA(cudaMemcpy(b.leaf_geometry.ptr, leaf.data(), leaf.size() * 4, cudaMemcpyHostToDevice), "upload batch leaf indices");
+    if (!emis.empty())
+        SLIM_CUDA(cudaMemcpy(b.emissive.ptr, emis.data(), emis.size() * 4, cudaMemcpyHostToDevice), "upload batch emissive lists");
+    SLIM_CUDA(cudaMemcpy(b.scenes.ptr, b.h_scenes.data(), count * sizeof(DevScene), cudaMemcpyHostToDevice), "upload batch scene table");
+    SLIM_CUDA(cudaMemcpy(b.frames.ptr, b.h_frames.data(), count * sizeof(DevFrame), cudaMemcpyHostToDevice), "upload batch frame table");
+    if (!b.plan.queue_capacity) {
+        b.plan.queue_capacity = 4u << 20;
+        b.plan.tile_pixels = 1u << 16;
+        b.plan.block_size = 256;
+    }
+    return batch_prepare(c, b);
+}
+
+int slimBatchSetPlan(const SlimBatchPlan *plan) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!plan || plan->queue_capacity < 1024 || plan->queue_capacity > (1u << 26) || !plan->tile_pixels ||
+        plan->block_size < 0 || plan->block_size > 256 || (plan->block_size % 32))
+        return set_error(SLIM_ERR_ARGUMENT, "bad batch plan");
+    BatchState &b = g_batch;
+    b.drop_graph();
+    b.plan.queue_capacity = plan->queue_capacity;
+    b.plan.tile_pixels = plan->tile_pixels;
+    b.plan.block_size = plan->block_size;
+    b.plan.tuned = 0;
+    b.plan.batch_ms = 0;
+    b.plan.candidates = 0;
+    if (b.requests.empty()) return SLIM_OK;
+    return batch_prepare(g_ctx, b);
+}
+
+int slimBatchGetPlan(SlimBatchPlan *plan) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!plan) return set_error(SLIM_ERR_ARGUMENT, "plan is null");
+    *plan = g_batch.plan;
+    plan->graph_nodes = (uint32_t)g_batch.graph_nodes;
+    return SLIM_OK;
+}
+
+// Coordinate search: queue capacity first (the wave size sets the number of
+// waves, the depth of the small late-bounce queues and the memory), then the
+// block size, then the tile size that packs requests into waves.
+int slimBatchTune(void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    BatchState &b = g_batch;
+    if (b.requests.empty()) return set_error(SLIM_ERR_STATE, "slimBatchSetRequests has not been called");
+    b.drop_graph();
+    cudaStream_t s = (cudaStream_t)stream;
+    SlimBatchPlan best = b.plan;
+    if (!best.queue_capacity) { best.queue_capacity = 4u << 20; best.tile_pixels = 1u << 16; best.block_size = 256; }
+    float best_ms = 1e30f;
+    uint32_t tried = 0;
+    auto attempt = [&](uint32_t Q, uint32_t T, int block) -> int {
+        b.plan.queue_capacity = Q;
+        b.plan.tile_pixels = T;
+        b.plan.block_size = block;
+        float ms = 0;
+        int rc = batch_time(c, b, s, 2, ms);
+        if (rc) return rc;
+        tried++;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = b.plan;
+        }
+        return SLIM_OK;
+    };
+    uint64_t total = b.pixels;
+    int rc;
+    const SlimBatchPlan before = b.plan;
+    auto fail = [&](int code) { b.plan = before; batch_prepare(c, b); return code; };
+    for (uint32_t Q : {1u << 20, 2u << 20, 4u << 20, 8u << 20, 16u << 20}) {
+        if (Q > 2 * total && Q != (1u << 20)) break;    // one wave already holds everything
+        if ((rc = attempt(Q, best.tile_pixels, best.block_size))) return fail(rc);
+    }
+    for (int block : {128, 256})
+        if (block != best.block_size && (rc = attempt(best.queue_capacity, best.tile_pixels, block))) return fail(rc);
+    for (uint32_t T : {1u << 14, 1u << 18})
+        if ((rc = attempt(best.queue_capacity, T, best.block_size))) return fail(rc);
+    b.plan = best;
+    b.plan.batch_ms = best_ms;
+    b.plan.candidates = tried;
+    b.plan.tuned = 1;
+    return batch_prepare(c, b);
+}
+
+int slimBatchRender(void *stream) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    BatchState &b = g_batch;
+    if (b.requests.empty()) return set_error(SLIM_ERR_STATE, "slimBatchSetRequests has not been called");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b.graph_valid) {
+        // a capture needs a non-default stream
+        cudaStream_t cap = s;
+        cudaStream_t own = nullptr;
+        if (!cap) {
+            SLIM_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking), "batch capture stream");
+            cap = own;
+        }
+        SLIM_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin batch capture");
+        const unsigned long long launched = g_kernel_launches.load();
+        int rc = batch_launch(c, b, cap);
+        g_kernel_launches.store(launched);    // recorded, not run: replays count the graph's kernels
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cap, &graph);
+        if (own) cudaStreamDestroy(own);
+        if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "end batch capture");
+        b.graph = graph;
+        SLIM_CUDA(cudaGraphInstantiate(&b.exec, graph, 0), "instantiate batch graph");
+        size_t nodes = 0;
+        cudaGraphGetNodes(graph, nullptr, &nodes);
+        std::vector<cudaGraphNode_t> list(nodes);
+        if (nodes) cudaGraphGetNodes(graph, list.data(), &nodes);
+        size_t kernels = 0;
+        for (cudaGraphNode_t n : list) {
+            cudaGraphNodeType type;
+            if (cudaGraphNodeGetType(n, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) kernels++;
+        }
+        b.graph_nodes = kernels;
+        b.graph_valid = true;
+    }
+    SLIM_CUDA(cudaGraphLaunch(b.exec, s), "launch batch graph");
+    count_launch(b.graph_nodes);
     return SLIM_OK;
 }
 

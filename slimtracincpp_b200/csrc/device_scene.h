@@ -76,6 +76,7 @@ struct DevFrame {
     float *depths;
     uint32_t *error_flags;
     unsigned long long *counters;  // SlimWorkCounters fields, or null
+    uint32_t cache_depth;          // batched requests: path vertex answered by the radiance cache (0 = none)
 };
 
 }  // namespace slim

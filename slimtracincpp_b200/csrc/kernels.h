@@ -1,6 +1,7 @@
 // Launchers of the trace kernels (implemented in kernels_*.cu).
 #pragma once
 #include <cuda_runtime.h>
+#include "launch_count.h"
 #include "device_scene.h"
 
 namespace slim {
@@ -66,14 +67,51 @@ struct CacheFrame {
     uint32_t *counts = nullptr;    // [0] queries, [1] training paths
     uint32_t train_capacity = 0;   // training paths per frame (every query in EXACT mode)
     float4 *t_features = nullptr, *t_targets = nullptr, *t_color = nullptr, *t_through = nullptr;
-    float select_offset = 0.0f;    // stratified selection offset in [0,1)
+    uint32_t *frame_counter = nullptr;  // device: cache frames so far (moves the stratified
+                                        // selection from frame to frame; counted on the device
+                                        // so captured graphs replay correctly)
     uint32_t batch = 0;            // samples per training step
     const uint8_t *weights = nullptr;   // bf16 weight image
     CacheTrainer *trainer = nullptr;    // null: no training this frame
+    // Overlapped training (ON mode with a trainer): the training paths of this
+    // frame are traced and trained on `train_stream` with their own queues,
+    // while the frame's stream answers the queries with the weights trained
+    // through the previous frame.  The frame's stream waits for the previous
+    // frame's training (`trained`) before it selects new training paths and
+    // before it queries the network; `selected` hands the new set over.
+    cudaStream_t train_stream = nullptr;      // null: train in order on the frame's stream
+    cudaEvent_t selected = nullptr, trained = nullptr;
+    const WavefrontBuffers *train_queues = nullptr;
+    const uint8_t *train_weights = nullptr;   // image the training updates; copied into `weights`
+                                              // (what the queries read) once per frame
 };
 
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
                                     cudaStream_t stream, StageTimer *timer, const CacheFrame *cache = nullptr);
+
+// Batched requests (no counterpart in the reference): many requests, each
+// with its own scene, camera and canvas, traced together over one set of
+// queues.  Their pixels are cut into tiles; consecutive tiles fill waves of
+// at most the queue capacity, and every wave is one multi-request frame
+// whose stage kernels look up each path's scene and canvas by request.
+struct BatchWave {
+    uint32_t first_tile, tile_count;   // into BatchFrame::tiles
+    uint32_t samples;                  // path slots of the wave
+    uint32_t max_depth, max_lights;    // over the wave's requests
+    uint32_t cache_paths;              // non-zero: a request of the wave uses the radiance cache
+};
+struct BatchFrame {
+    DevScene shared;                   // mesh and texture arrays every request shares
+    DevFrame frame;                    // error flags and counters every request shares
+    const DevScene *scenes;            // device table, one entry per request
+    const DevFrame *frames;            // device table, one entry per request
+    const uint4 *tiles;                // device: (request, first pixel, pixel count, first slot in its wave)
+    const BatchWave *waves;            // host
+    uint32_t wave_count;
+    const CacheFrame *cache;           // null: no request uses the cache
+};
+cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
+                                StageTimer *timer);
 
 // GPU refit of the scene BVH: recomputes every node's bounds bottom-up from
 // the geometries' world AABBs, keeping the uploaded topology.

@@ -171,8 +171,13 @@ cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block,
     if (block > 128) block = 128;
     dim3 grid((n + block - 1) / block);
     if (timer) timer->begin(STAGE_FUSED, stream);
-    if (F.counters) dev::k_render_fused<true><<<grid, block, 0, stream>>>(S, F);
-    else dev::k_render_fused<false><<<grid, block, 0, stream>>>(S, F);
+    if (F.counters) {
+        dev::k_render_fused<true><<<grid, block, 0, stream>>>(S, F);
+        count_launch();
+    } else {
+        dev::k_render_fused<false><<<grid, block, 0, stream>>>(S, F);
+        count_launch();
+    }
     if (timer) timer->end(STAGE_FUSED, stream);
     return cudaGetLastError();
 }
@@ -184,6 +189,7 @@ cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjectio
     dim3 grid((n + 127) / 128);
     dev::k_trace_primary<<<grid, 128, 0, stream>>>(S, P, width, height, geometry_ids, primitive_ids, distances,
                                                   from_behind, error_flags);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(128, 1) k_nrc_train(const float4 *__restrict__
                                                       const uint32_t *count, uint32_t offset,
                                                       const uint8_t *__restrict__ weight_image,
                                                       float *__restrict__ partials, float *__restrict__ loss_partials,
-                                                      uint32_t *error_flags) {
+                                                      uint32_t *step, uint32_t *error_flags) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t *W = smem;
     uint8_t *X = W + kImgBytes;
@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(128, 1) k_nrc_train(const float4 *__restrict__
     const uint32_t t = threadIdx.x, warp = t >> 5;
     const uint32_t n = step_samples(n_max, count, offset);
     const uint32_t tiles = (n + kTile - 1) / kTile;
+    if (n && blockIdx.x == 0 && t == 0) atomicAdd(step, 1u);
     features += 4 * (size_t)offset;
     targets += offset;
     for (uint32_t i = t; i < kImgBytes / 16; i += blockDim.x)
@@ -478,6 +479,8 @@ __global__ void k_nrc_adam(float *__restrict__ params, float *__restrict__ m, fl
     const uint32_t n = step_samples(n_max, count, offset);
     if (!n) return;                                  // empty step: no update
     const float scale = 1.0f / (3.0f * (float)n);
+    const float t = (float)*a.step;
+    const float bias1 = 1.0f / (1.0f - powf(a.beta1, t)), bias2 = 1.0f / (1.0f - powf(a.beta2, t));
     if (p == 0) {
         float s = 0.0f;
         for (uint32_t b = 0; b < a.parts; b++) s += loss_partials[b];
@@ -492,7 +495,7 @@ __global__ void k_nrc_adam(float *__restrict__ params, float *__restrict__ m, fl
     float vv = a.beta2 * v[p] + (1.0f - a.beta2) * g * g;
     m[p] = mm;
     v[p] = vv;
-    float w = params[p] - a.lr * (mm * a.bias1) / (sqrtf(vv * a.bias2) + a.eps);
+    float w = params[p] - a.lr * (mm * bias1) / (sqrtf(vv * bias2) + a.eps);
     params[p] = w;
     *(unsigned short *)(image + param_offset(p)) = (unsigned short)bf16_bits(w);
 }
@@ -520,20 +523,21 @@ int train_grid(uint32_t samples) {
     return (int)(tiles < g ? (tiles ? tiles : 1) : g);
 }
 
+cudaError_t prepare() {
+    cudaError_t e = cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
+}
+
 cudaError_t launch_infer(const float4 *features, const uint32_t *count, uint32_t n, uint32_t capacity, float4 *radiance,
                          const uint8_t *weight_image, uint32_t *error_flags, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
     uint32_t bound = count ? capacity : n;
     uint32_t tiles = (bound + kTile - 1) / kTile;
     if (!tiles) return cudaSuccess;
     uint32_t g = 2u * (uint32_t)sm_count();
     if (tiles < g) g = tiles;
     k_nrc_infer<<<g, 128, kInferSmem, stream>>>(features, count, n, radiance, weight_image, error_flags);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -541,20 +545,16 @@ cudaError_t launch_train_step(const float4 *features, const float4 *targets, uin
                               uint32_t offset, float *params, float *adam_m, float *adam_v, uint8_t *weight_image,
                               float *partials, float *loss_partials, float *grad, float *loss, const AdamArgs &adam,
                               uint32_t *error_flags, cudaStream_t stream) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
     if (!samples) return cudaSuccess;
     int g = train_grid(samples);
     k_nrc_train<<<g, 128, kTrainSmem, stream>>>(features, targets, samples, count, offset, weight_image, partials,
-                                                 loss_partials, error_flags);
+                                                 loss_partials, adam.step, error_flags);
+    count_launch();
     AdamArgs a = adam;
     a.parts = (uint32_t)g;
     k_nrc_adam<<<(kParams + 255) / 256, 256, 0, stream>>>(params, adam_m, adam_v, partials, loss_partials, grad, loss,
                                                           weight_image, a, samples, count, offset);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -562,6 +562,7 @@ cudaError_t launch_pack_weights(const float *params, uint8_t *weight_image, cuda
     cudaError_t e = cudaMemsetAsync(weight_image, 0, kImgBytes, stream);
     if (e != cudaSuccess) return e;
     k_nrc_pack<<<(kParams + 255) / 256, 256, 0, stream>>>(params, weight_image);
+    count_launch();
     return cudaGetLastError();
 }
 

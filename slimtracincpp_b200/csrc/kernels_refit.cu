@@ -79,7 +79,11 @@ cudaError_t launch_refit_scene_bvh(const DevScene &S, float4 *scene_nodes, const
     if (!n) return cudaSuccess;
     if (timer) timer->begin(STAGE_REFIT, stream);
     dev::k_refit_leaves<<<(n + 127) / 128, 128, 0, stream>>>(S, scene_nodes, n);
-    if (inner_count) dev::k_refit_inner<<<1, 1, 0, stream>>>(scene_nodes, order, inner_count);
+    count_launch();
+    if (inner_count) {
+        dev::k_refit_inner<<<1, 1, 0, stream>>>(scene_nodes, order, inner_count);
+        count_launch();
+    }
     if (timer) timer->end(STAGE_REFIT, stream);
     return cudaGetLastError();
 }

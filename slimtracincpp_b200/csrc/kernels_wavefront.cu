@@ -79,6 +79,17 @@ SLIM_D void flush_stage(unsigned long long *counters, const Work &w) {
     }
 }
 
+// Radiance-cache state of a frame (see kernels.h CacheFrame).
+struct CacheArgs {
+    float4 *features, *aux, *radiance;
+    uint32_t *count;               // queries
+    uint32_t *train_count;         // training paths
+    uint32_t train_capacity;
+    float4 *t_features, *t_targets, *t_color, *t_through;
+    uint32_t *frame_counter;
+    int mode;
+};
+
 struct QueueArgs {
     const float4 *rays_in;        // null: primary rays generated from the slot (= sample index)
     float4 *rays_out;
@@ -93,8 +104,8 @@ struct QueueArgs {
     uint32_t *pair_count;
     uint32_t *pair_cursor;
     uint32_t pair_capacity;
-    float4 *path_color;           // per sample: colour, depth
-    float4 *path_throughput;      // per sample: throughput
+    float4 *path_color;           // per path: colour, depth
+    float4 *path_throughput;      // per path: throughput
     uint32_t samples;
     uint32_t depth;               // 1-based bounce of this round
     uint32_t light_begin, light_end;
@@ -103,7 +114,32 @@ struct QueueArgs {
     float4 *sink;                 // non-null: finished paths write their linear colour here
                                   // (indexed by the path slot) instead of the canvas
     uint32_t skip_glow_depth;     // no light glow on the segment of this depth (0 = none)
+    CacheArgs cache;              // batched frames: queries of requests using the cache
+    // batched requests (null in a single-request frame)
+    const DevScene *scenes;
+    const DevFrame *frames;
 };
+
+// Ray records: (origin.xyz, path) (direction.xyz, pid).  `path` indexes the
+// path state (colour, throughput); `pid` names the canvas pixel: the pixel
+// index in a single-request frame, (request << 23) | pixel in a batch.  The
+// two differ for the radiance cache's training paths, whose state lives in
+// their own slots, and for batched paths, whose slots are per wave.
+constexpr uint32_t kBatchPixelBits = 23;
+constexpr uint32_t kBatchMaxRequests = 1u << (32 - kBatchPixelBits);
+
+template <bool BATCH> SLIM_D uint32_t req_of(uint32_t pid) { return BATCH ? pid >> kBatchPixelBits : 0u; }
+template <bool BATCH> SLIM_D uint32_t pix_of(uint32_t pid) {
+    return BATCH ? pid & ((1u << kBatchPixelBits) - 1u) : pid;
+}
+template <bool BATCH> SLIM_D const DevScene &scene_of(const DevScene &S, const QueueArgs &A, uint32_t pid) {
+    if constexpr (BATCH) return A.scenes[req_of<true>(pid)];
+    else return S;
+}
+template <bool BATCH> SLIM_D const DevFrame &frame_of(const DevFrame &F, const QueueArgs &A, uint32_t pid) {
+    if constexpr (BATCH) return A.frames[req_of<true>(pid)];
+    else return F;
+}
 
 SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
     int x = (int)(i % F.width), y = (int)(i / F.width);
@@ -112,58 +148,64 @@ SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
     d = normalized(primary_direction(P, x, y));
 }
 
-// `pixel` indexes the path state (and the canvas); `cone_pixel` is the canvas
-// pixel whose ray-cone spread the path uses.  They differ only for the
-// radiance cache's training paths, whose state lives in their own slots.
-SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel,
-                     uint32_t &cone_pixel) {
+SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &path,
+                     uint32_t &pid) {
     if (!A.rays_in) {
-        pixel = cone_pixel = slot;
+        path = pid = slot;
         primary_ray(F, slot, o, d);
         return;
     }
     float4 a = A.rays_in[2 * (size_t)slot], b = A.rays_in[2 * (size_t)slot + 1];
     o = xyz(a);
-    pixel = __float_as_uint(a.w);
+    path = __float_as_uint(a.w);
     d = xyz(b);
-    cone_pixel = __float_as_uint(b.w);
+    pid = __float_as_uint(b.w);
 }
-SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &pixel) {
-    uint32_t cone_pixel;
-    load_ray(F, A, slot, o, d, pixel, cone_pixel);
+template <bool BATCH> SLIM_D float cone_scaling(const DevFrame &F, uint32_t pid) {
+    uint32_t p = pix_of<BATCH>(pid);
+    return F.cones_per_pixel ? pixel_scaling(F.projection, (int)(p % F.width), (int)(p / F.width)) : 0.0f;
 }
-SLIM_D float cone_scaling(const DevFrame &F, uint32_t cone_pixel) {
-    return F.cones_per_pixel ? pixel_scaling(F.projection, (int)(cone_pixel % F.width), (int)(cone_pixel / F.width))
-                             : 0.0f;
+template <bool BATCH> SLIM_D void write_pixel(const DevFrame &F, uint32_t pid, float3 color, float depth) {
+    uint32_t p = pix_of<BATCH>(pid);
+    float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
+    set_pixel(F, (int)(p % F.width), (int)(p / F.width), c, depth);
 }
 
 SLIM_D uint32_t queue_size(const QueueArgs &A) { return A.count_in ? *A.count_in : A.samples; }
 
 // ---- extend: closest hit of every queued ray ----------------------------
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_extend(DevScene S, DevFrame F, QueueArgs A) {
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
     uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
     uint32_t err = 0;
     Work w = {};
     for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
         float3 o, d;
-        uint32_t pixel;
-        load_ray(F, A, slot, o, d, pixel);
+        uint32_t path, pid;
+        load_ray(F0, A, slot, o, d, path, pid);
         if (!A.rays_in) bump<COUNT>(w.primary);
+        const DevScene &S = scene_of<BATCH>(S0, A, pid);
         Ray ray;
         reset(ray, o, d);
         Hit hit;
         int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
         store_hit(A.hits, slot, g, hit);
     }
-    if (err) atomicOr(F.error_flags, err);
+    if (err) atomicOr(F0.error_flags, err);
     flush_stage<COUNT>(A.counters, w);
 }
 
+// A batched request's path that reached its radiance-cache vertex: the
+// cache answers there, so it is neither shaded nor lit (training paths,
+// which carry a sink, are).
+template <bool BATCH> SLIM_D bool at_cache_vertex(const DevFrame &F, const QueueArgs &A) {
+    return BATCH && F.cache_depth == A.depth && !A.sink;
+}
+
 // ---- shadow_gen: one shadow ray per facing, shadowing light -------------
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, QueueArgs A) {
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
     Work w = {};
     uint32_t stride = gridDim.x * blockDim.x;
@@ -174,28 +216,32 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S, DevFrame F, Queu
         bool live = slot < n;
         Surface s;
         bool shaded = false;
+        uint32_t lights = 0, pid = 0;
         if (live) {
             if (A.light_begin == 0) A.masks[slot] = 0ull;
             float3 o, d;
-            uint32_t pixel, cone_pixel;
-            load_ray(F, A, slot, o, d, pixel, cone_pixel);
+            uint32_t path;
+            load_ray(F0, A, slot, o, d, path, pid);
+            const DevScene &S = scene_of<BATCH>(S0, A, pid);
+            const DevFrame &F = frame_of<BATCH>(F0, A, pid);
+            lights = S.light_count;
             Hit hit;
             int g = load_hit(A.hits, slot, hit);
-            if (g >= 0) {
+            if (g >= 0 && !at_cache_vertex<BATCH>(F, A)) {
                 Geo geo = load_geo(S, (uint32_t)g);
                 Mat m = load_mat(S, geo.material);
                 if (!((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind)) {
                     Ray ray;
                     reset(ray, scale_add(d, kTraceOffset, o), d);
-                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
+                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
                     shaded = true;
                 }
             }
         }
         for (uint32_t li = A.light_begin; li < A.light_end; li++) {
             bool want = false;
-            if (shaded) {
-                LightRec l = load_light(S, li);
+            if (shaded && li < lights) {
+                LightRec l = load_light(scene_of<BATCH>(S0, A, pid), li);
                 want = is_facing_light(s, l) && (l.flags & SLIM_LIGHT_IS_SHADOWING);
             }
             uint32_t q = warp_append(A.shadow_count, want);
@@ -292,8 +338,8 @@ SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t tag, uin
     return false;
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow_scene(DevScene S, DevFrame F, QueueArgs A) {
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_shadow_scene(DevScene S0, DevFrame F, QueueArgs A) {
     uint32_t n = *A.shadow_count;
     uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
     uint32_t err = 0;
@@ -301,6 +347,7 @@ __global__ void __launch_bounds__(256) k_shadow_scene(DevScene S, DevFrame F, Qu
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         float4 a = A.shadow_rays[2 * (size_t)q], b = A.shadow_rays[2 * (size_t)q + 1];
         uint32_t tag = __float_as_uint(a.w);
+        const DevScene &S = scene_of<BATCH>(S0, A, BATCH ? __float_as_uint(A.rays_in[2 * (size_t)(tag >> 6) + 1].w) : 0u);
         Ray ray;
         float3 d = xyz(b);
         reset(ray, scale_add(d, kTraceOffset, xyz(a)), d);
@@ -434,174 +481,515 @@ __global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, Que
     flush_stage<COUNT>(A.counters, w);
 }
 
-// ---- shade: colour of this segment, next bounce, finished paths --------
-template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shade(DevScene S, DevFrame F, QueueArgs A) {
+
+// ---- extend, split: closest hit as scene candidates + a persistent mesh pass
+//
+// The closest hit the reference's SceneTracer::trace finds is the candidate
+// with the smallest distance, ties going to the one it visits first: a later
+// candidate replaces the current hit only when strictly closer
+// (scene_tracer.h:129, mesh_tracer.h:37).  Culling by the current distance
+// only skips candidates that cannot win, and a mesh walk started with a
+// larger incoming distance finds a superset of hits in the same visiting
+// order.  So the search splits exactly:
+//   extend_scene   walks the scene BVH in the reference's order, numbering
+//                  every geometry it visits (k), tests implicit primitives on
+//                  the spot (culling by the best implicit hit so far) and
+//                  appends one candidate per reached mesh instance;
+//   extend_mesh    a persistent kernel: every lane takes one mesh-BVH step
+//                  per loop turn in the reference's order and fetches the
+//                  next candidate when its walk ends; finished candidates
+//                  publish (distance, k) with a 64-bit atomicMin per ray;
+//   extend_resolve the candidate whose (distance, k) is the ray's minimum
+//                  writes the hit record.
+// Cross-candidate culling keeps ties (<=), so the winner is the reference's.
+// Candidate records (4 float4): (local origin, clip) (local direction, slot)
+// (node offset, triangle offset, first child, 0) (geometry, mesh, k, found);
+// a finished walk overwrites the third with (t, u, v, triangle | behind << 31)
+// and sets `found`.  The ray keys live in the shadow-mask array, which is
+// free until the shadow stage.
+
+SLIM_D unsigned long long hit_key(float t, uint32_t k) {
+    return ((unsigned long long)__float_as_uint(t) << 32) | k;
+}
+constexpr unsigned long long kNoHitKey = ~0ull;
+
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend_scene(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
+    uint32_t stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    const uint32_t cap = A.pair_capacity * 3u / 4u;
+    uint32_t *overflow = reinterpret_cast<uint32_t *>(A.shadow_rays);   // free until shadow_gen
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        float3 o, d;
+        uint32_t path, pid;
+        load_ray(F0, A, slot, o, d, path, pid);
+        if (!A.rays_in) bump<COUNT>(w.primary);
+        const DevScene &S = scene_of<BATCH>(S0, A, pid);
+        Ray r;
+        reset(r, scale_add(d, kTraceOffset, o), d);
+        Hit hit;
+        hit.distance = INFINITY;
+        int best_geo = -1;
+        uint32_t best_k = 0, k = 0;
+        bool full = false;
+        // one scene leaf: [first, first + count) geometries, far distance lf
+        auto leaf = [&](uint32_t first, uint32_t count, float lf) {
+            Hit aux;
+            aux.distance = minr(lf + kEps, hit.distance);
+            const float clip = lf + kEps;
+            Ray local;
+            for (uint32_t i = 0; i < count; i++, k++) {
+                uint32_t gi = __ldg(S.leaf_geometry + first + i);
+                Geo g = load_geo(S, gi);
+                if (!(g.flags & SLIM_GEOMETRY_IS_VISIBLE)) continue;
+                if (g.type != SLIM_GEOMETRY_MESH) {
+                    if (hit_geometry_local<COUNT>(S, g, r, local, aux, false, nullptr, err, w) &&
+                        aux.distance < hit.distance) {
+                        best_geo = (int)gi;
+                        best_k = k;
+                        hit = aux;
+                        hit.NdotRd = -(dot(hit.normal, local.d));
+                    }
+                    continue;
+                }
+                bump<COUNT>(w.geometries);
+                localize(local, r.o, r.d, g);
+                const DevMesh &m = S.meshes[g.mesh];
+                float bn, bf;
+                if (!hit_aabb(local, m.aabb_min[0], m.aabb_min[1], m.aabb_min[2], m.aabb_max[0], m.aabb_max[1],
+                              m.aabb_max[2], bn, bf))
+                    continue;
+                const float4 *nodes = S.mesh_nodes + 2 * (size_t)m.node_offset;
+                float4 ra, rb;
+                float rn, rf;
+                load_node(nodes, 0, ra, rb);
+                bump<COUNT>(w.mesh_nodes);
+                // the root test with the largest distance the reference could have used
+                if (!(hit_node(local, ra, rb, rn, rf) && rn < clip && rn <= hit.distance)) continue;
+                if (node_leaf_count(rb)) {
+                    // a single-leaf mesh (mesh_tracer.h:66-70): its triangles here
+                    Hit mh;
+                    mh.distance = clip;
+                    if (hit_triangles<COUNT>(S.tri_hot, m.tri_offset, m.tri_count, rf, local, mh, false, w) &&
+                        mh.distance < hit.distance) {
+                        mh.uv_coverage = __ldg(&S.tri_cold[4 * (size_t)(m.tri_offset + mh.id) + 3].w);
+                        best_geo = (int)gi;
+                        best_k = k;
+                        hit = mh;
+                        hit.NdotRd = -(dot(hit.normal, local.d));
+                    }
+                    continue;
+                }
+                uint32_t q = warp_append(A.pair_count, true);
+                if (q >= cap) { full = true; continue; }
+                float4 *p = A.pairs + 4 * (size_t)q;
+                p[0] = make_float4(local.o.x, local.o.y, local.o.z, clip);
+                p[1] = make_float4(local.d.x, local.d.y, local.d.z, __uint_as_float(slot));
+                p[2] = make_float4(__uint_as_float(m.node_offset), __uint_as_float(m.tri_offset),
+                                   __uint_as_float(node_first(rb)), 0.0f);
+                p[3] = make_float4(__uint_as_float(gi), __uint_as_float(g.mesh), __uint_as_float(k), 0.0f);
+            }
+        };
+        float ln, rn, lf, rf;
+        float4 a, b;
+        load_node(S.scene_nodes, 0, a, b);
+        bump<COUNT>(w.scene_nodes);
+        if (hit_node(r, a, b, ln, lf) && ln < hit.distance) {
+            if (node_leaf_count(b)) {
+                leaf(0, S.geometry_count, lf);
+            } else {
+                uint32_t left = node_first(b), top = 0;
+                for (;;) {
+                    float4 la, lb, xa, xb;
+                    load_node(S.scene_nodes, left, la, lb);
+                    load_node(S.scene_nodes, left + 1, xa, xb);
+                    bump<COUNT>(w.scene_nodes, 2);
+                    bool hl = hit_node(r, la, lb, ln, lf) && ln < hit.distance;
+                    bool hr = hit_node(r, xa, xb, rn, rf) && rn < hit.distance;
+                    uint32_t lchild = node_first(lb), rchild = node_first(xb);
+                    bool go_left = hl, go_right = hr;
+                    if (hl && node_leaf_count(lb)) {
+                        leaf(lchild, node_leaf_count(lb), lf);
+                        go_left = false;
+                    }
+                    if (hr && node_leaf_count(xb)) {
+                        leaf(rchild, node_leaf_count(xb), rf);
+                        go_right = false;
+                    }
+                    if (go_left) {
+                        if (go_right) {
+                            if (ln > rn) { uint32_t t = lchild; lchild = rchild; rchild = t; }
+                            if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; break; }
+                            stack[top++] = rchild;
+                        }
+                        left = lchild;
+                    } else if (go_right) {
+                        left = rchild;
+                    } else {
+                        if (top == 0) break;
+                        left = stack[--top];
+                    }
+                }
+            }
+        }
+        if (full) {
+            // the candidate queue ran out: the ray is traced whole afterwards
+            // (k_extend_overflow); key 0 matches no candidate (hit distances
+            // are never 0: the plane test rejects an origin on the plane)
+            A.masks[slot] = 0ull;
+            overflow[atomicAdd(A.pair_count + 2, 1u)] = slot;
+        } else {
+            A.masks[slot] = best_geo >= 0 ? hit_key(hit.distance, best_k) : kNoHitKey;
+            store_hit(A.hits, slot, best_geo, hit);
+        }
+    }
+    if (err) atomicOr(F0.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// Rays whose candidates did not fit: the reference's whole closest-hit walk.
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend_overflow(DevScene S0, DevFrame F0, QueueArgs A) {
+    const uint32_t n = A.pair_count[2];
+    const uint32_t *overflow = reinterpret_cast<const uint32_t *>(A.shadow_rays);
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = overflow[i];
+        float3 o, d;
+        uint32_t path, pid;
+        load_ray(F0, A, slot, o, d, path, pid);
+        const DevScene &S = scene_of<BATCH>(S0, A, pid);
+        Ray ray;
+        reset(ray, o, d);
+        Hit hit;
+        int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+        store_hit(A.hits, slot, g, hit);
+    }
+    if (err) atomicOr(F0.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_extend_mesh(DevScene S, DevFrame F, QueueArgs A) {
+    const uint32_t cap = A.pair_capacity * 3u / 4u;
+    const uint32_t n = *A.pair_count < cap ? *A.pair_count : cap;
+    uint32_t stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    bool busy = false;
+    uint32_t idx = 0, slot = 0, left = 0, top = 0, tri_offset = 0, tri = 0, k = 0;
+    const float4 *nodes = nullptr;
+    float lc = 0.0f, bu = 0.0f, bv = 0.0f;
+    bool found = false, behind = false;
+    Ray r;
+    for (;;) {
+        if (!busy) {
+            uint32_t active = __activemask();
+            int leader = __ffs(active) - 1;
+            uint32_t base = 0;
+            if ((int)lane_id() == leader) base = atomicAdd(A.pair_cursor, (uint32_t)__popc(active));
+            base = __shfl_sync(active, base, leader);
+            idx = base + (uint32_t)__popc(active & ((1u << lane_id()) - 1u));
+            if (idx >= n) break;
+            const float4 *p = A.pairs + 4 * (size_t)idx;
+            float4 p0 = p[0], p1 = p[1], p2 = p[2];
+            reset(r, xyz(p0), xyz(p1));
+            lc = p0.w;
+            slot = __float_as_uint(p1.w);
+            k = __float_as_uint(p[3].z);
+            nodes = S.mesh_nodes + 2 * (size_t)__float_as_uint(p2.x);
+            tri_offset = __float_as_uint(p2.y);
+            left = __float_as_uint(p2.z);
+            top = 0;
+            found = false;
+            busy = true;
+        }
+        // one step of MeshTracer::trace (mesh_tracer.h:51-114), closest hit
+        const float gb = __uint_as_float((uint32_t)(A.masks[slot] >> 32));   // best of the ray so far (may lag)
+        float ln, rn, lf, rf;
+        float4 la, lb, xa, xb;
+        load_node(nodes, left, la, lb);
+        load_node(nodes, left + 1, xa, xb);
+        bump<COUNT>(w.mesh_nodes, 2);
+        bool hl = hit_node(r, la, lb, ln, lf) && ln < lc && ln <= gb;
+        bool hr = hit_node(r, xa, xb, rn, rf) && rn < lc && rn <= gb;
+        uint32_t lchild = node_first(lb), rchild = node_first(xb);
+        bool go_left = hl, go_right = hr;
+        for (int side = 0; side < 2; side++) {
+            const bool h = side ? hr : hl;
+            const uint32_t first = side ? rchild : lchild;
+            const uint32_t count = node_leaf_count(side ? xb : lb);
+            if (!h || !count) continue;
+            if (side) go_right = false; else go_left = false;
+            // MeshTracer::hitTriangles (mesh_tracer.h:23-49) with the leaf's far clip
+            float closest = minr(side ? rf : lf, lc);
+            for (uint32_t i = 0; i < count; i++) {
+                bump<COUNT>(w.triangles);
+                const float4 *t4 = S.tri_hot + 3 * (size_t)(tri_offset + first + i);
+                float4 a = __ldg(t4), b = __ldg(t4 + 1), c = __ldg(t4 + 2);
+                float3 pp = xyz(a), nn = f3(a.w, b.x, b.y);
+                float tt; float3 pos; bool bh;
+                if (!hit_plane(r, pp, nn, tt, pos, bh)) continue;
+                float3 q = pos - pp;
+                float ux = b.z * q.x + c.x * q.y + c.z * q.z;
+                float uy = b.w * q.x + c.y * q.y + c.w * q.z;
+                if (ux < 0 || uy < 0 || (ux + uy) > 1 || tt >= closest || tt > gb) continue;
+                closest = tt;
+                lc = tt;
+                bu = ux;
+                bv = uy;
+                behind = bh;
+                tri = first + i;
+                found = true;
+            }
+        }
+        int res = 0;
+        if (go_left) {
+            if (go_right) {
+                if (ln > rn) { uint32_t t = lchild; lchild = rchild; rchild = t; }
+                if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; res = -1; }
+                else stack[top++] = rchild;
+            }
+            left = lchild;
+        } else if (go_right) {
+            left = rchild;
+        } else if (top == 0) {
+            res = -1;
+        } else {
+            left = stack[--top];
+        }
+        if (res) {
+            float4 *p = A.pairs + 4 * (size_t)idx;
+            if (found) {
+                p[2] = make_float4(lc, bu, bv, __uint_as_float(tri | ((uint32_t)behind << 31)));
+                atomicMin(A.masks + slot, hit_key(lc, k));
+            }
+            p[3].w = found ? 1.0f : 0.0f;
+            busy = false;
+        }
+    }
+    if (err) atomicOr(F.error_flags, err);
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// The candidate holding its ray's minimum (distance, k) writes the hit
+// record with the attributes MeshTracer::trace fills in.
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_extend_resolve(DevScene S0, DevFrame F0, QueueArgs A) {
+    const uint32_t cap = A.pair_capacity * 3u / 4u;
+    const uint32_t n = *A.pair_count < cap ? *A.pair_count : cap;
+    Work w = {};
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        const float4 *p = A.pairs + 4 * (size_t)idx;
+        const float4 p3 = p[3];
+        if (p3.w == 0.0f) continue;
+        const float4 p1 = p[1], p2 = p[2];
+        const uint32_t slot = __float_as_uint(p1.w);
+        if (A.masks[slot] != hit_key(p2.x, __float_as_uint(p3.z))) continue;
+        uint32_t pid = 0;
+        if (BATCH) pid = __float_as_uint(A.rays_in[2 * (size_t)slot + 1].w);
+        const DevScene &S = scene_of<BATCH>(S0, A, pid);
+        const DevMesh &m = S.meshes[__float_as_uint(p3.y)];
+        Hit h;
+        h.distance = p2.x;
+        h.u = p2.y;
+        h.v = p2.z;
+        const uint32_t tb = __float_as_uint(p2.w);
+        h.id = tb & 0x7FFFFFFFu;
+        h.from_behind = (tb >> 31) != 0;
+        const float4 *t4 = S.tri_hot + 3 * (size_t)(m.tri_offset + h.id);
+        const float4 a = __ldg(t4), b = __ldg(t4 + 1);
+        h.normal = f3(a.w, b.x, b.y);
+        h.position = f3(0, 0, 0);
+        mesh_hit_attributes<COUNT>(S, m, h, w);
+        h.NdotRd = -(dot(h.normal, xyz(p1)));
+        store_hit(A.hits, slot, (int)__float_as_uint(p3.x), h);
+    }
+    flush_stage<COUNT>(A.counters, w);
+}
+
+// ---- radiance-cache vertex ---------------------------------------------------
+// The path has reached the vertex the cache answers at.  Misses and emissive
+// quads finish it exactly as k_shade does; every other hit turns it into a
+// query: the segment's glow is added to the path colour now, the surface's
+// features (position in the scene box, roughness, direction, shading normal,
+// albedo) go to the network, and the path waits in path_color /
+// path_throughput for the answer.  Returns true for a query.
+template <bool COUNT, bool BATCH>
+SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &A, uint32_t slot, uint32_t path,
+                         uint32_t pid, float3 o, float3 d, float4 f[4], Work &w) {
     const SlimRayTracerSettings &st = F.settings;
+    Ray ray;
+    reset(ray, scale_add(d, kTraceOffset, o), d);
+    Hit hit;
+    int g = load_hit(A.hits, slot, hit);
+    float4 pc = A.path_color[path];
+    float3 color = xyz(pc), throughput = xyz(A.path_throughput[path]);
+    float3 current = f3(0, 0, 0);
+    float hit_distance = INFINITY;
+    bool query = false;
+    if (g >= 0) {
+        hit_distance = hit.distance;
+        Geo geo = load_geo(S, (uint32_t)g);
+        Mat m = load_mat(S, geo.material);
+        if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+            current = m.emission;
+        } else {
+            Surface s;
+            prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
+            hit_distance = hit.distance;
+            query = true;
+            // scene box -> [0,1]^3 (longest side), from the scene BVH root
+            float4 r0 = make_float4(0, 0, 0, 1), r1 = make_float4(1, 1, 0, 0);
+            if (S.scene_node_count) { r0 = S.scene_nodes[0]; r1 = S.scene_nodes[1]; }
+            const float ext = fmaxf(fmaxf(r0.w - r0.x, r1.x - r0.y), r1.y - r0.z);
+            const float inv = ext > 0.0f ? 1.0f / ext : 1.0f;
+            float3 p = (s.P - f3(r0.x, r0.y, r0.z)) * inv;
+            float3 al = m.albedo * s.albedo_from_map;
+            f[0] = make_float4(p.x, p.y, p.z, m.roughness);
+            f[1] = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
+            f[2] = make_float4(s.N.x, s.N.y, s.N.z, 0.0f);
+            f[3] = make_float4(al.x, al.y, al.z, 0.0f);
+        }
+    } else if (st.skybox_color_texture_id >= 0) {
+        current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+    }
+    add_glow(S, ray, hit_distance, current);
+    color = mul_add(current, throughput, color);
+    if (query) A.path_color[path] = make_float4(color.x, color.y, color.z, pc.w);
+    else write_pixel<BATCH>(F, pid, color, pc.w);
+    return query;
+}
+
+SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], float3 o, float3 d, uint32_t path,
+                         uint32_t pid) {
+    float4 *p = C.features + 4 * (size_t)q;
+    p[0] = f[0]; p[1] = f[1]; p[2] = f[2]; p[3] = f[3];
+    C.aux[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __uint_as_float(path));
+    C.aux[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(pid));
+}
+
+// ---- shade: colour of this segment, next bounce, finished paths --------
+template <bool COUNT, bool BATCH>
+__global__ void __launch_bounds__(256) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
+    uint32_t n = queue_size(A);
     Work w = {};
     uint32_t stride = gridDim.x * blockDim.x;
     uint32_t rounds = (n + stride - 1) / stride;
     for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
         bool live = slot < n;
-        bool bounce = false;
-        uint32_t pixel = 0, cone_pixel = 0;
+        bool bounce = false, query = false;
+        uint32_t path = 0, pid = 0;
+        float3 o = f3(0, 0, 0), d = f3(0, 0, 0);
         float3 bo = f3(0, 0, 0), bd = f3(0, 0, 0);
+        float4 feat[4];
         if (live) {
-            float3 o, d;
-            load_ray(F, A, slot, o, d, pixel, cone_pixel);
-            Ray ray;
-            reset(ray, scale_add(d, kTraceOffset, o), d);
-            Hit hit;
-            int g = load_hit(A.hits, slot, hit);
-            float4 pc = A.depth == 1 ? make_float4(0, 0, 0, INFINITY) : A.path_color[pixel];
-            float3 color = xyz(pc), throughput = A.depth == 1 ? f3(1, 1, 1) : xyz(A.path_throughput[pixel]);
-            float depth = pc.w;
-            float3 current = f3(0, 0, 0), next_throughput = f3(0, 0, 0);
-            float hit_distance = INFINITY;
-            if (g >= 0) {
-                hit_distance = hit.distance;
-                Geo geo = load_geo(S, (uint32_t)g);
-                Mat m = load_mat(S, geo.material);
-                if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
-                    current = m.emission;
-                } else {
-                    Surface s;
-                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
-                    hit_distance = hit.distance;
-                    if (A.depth == 1) depth = depth_at(F.projection, hit.position);
-                    unsigned long long occluded = A.masks[slot];
-                    for (uint32_t i = 0; i < S.light_count; i++) {
-                        LightRec l = load_light(S, i);
-                        if (!is_facing_light(s, l)) continue;
-                        if ((l.flags & SLIM_LIGHT_IS_SHADOWING) && ((occluded >> i) & 1ull)) continue;
-                        add_light(s, m, l, current);
-                    }
-                    if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
-                    if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
-                        s.L = s.N;
-                        s.NdotL = 1.0f;
-                        float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
-                        float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
-                        radiance_fraction(s, m);
-                        current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
-                    }
-                    if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && A.depth < st.max_depth) {
-                        float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
-                        next_throughput = s.refracted ? one_minus(Fr) : Fr;
-                        bounce = true;
-                        bo = hit.position;
-                        bd = s.RF;
-                        reset(ray, bo, bd);
-                    }
-                }
-            } else if (st.skybox_color_texture_id >= 0) {
-                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
-            }
-            if (A.depth != A.skip_glow_depth) add_glow(S, ray, hit_distance, current);
-            color = mul_add(current, throughput, color);
-            throughput = throughput * next_throughput;
-            if (bounce) {
-                A.path_color[pixel] = make_float4(color.x, color.y, color.z, depth);
-                A.path_throughput[pixel] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
-            } else if (A.sink) {
-                A.sink[pixel] = make_float4(color.x, color.y, color.z, 0.0f);
+            load_ray(F0, A, slot, o, d, path, pid);
+            const DevScene &S = scene_of<BATCH>(S0, A, pid);
+            const DevFrame &F = frame_of<BATCH>(F0, A, pid);
+            const SlimRayTracerSettings &st = F.settings;
+            if (at_cache_vertex<BATCH>(F, A)) {
+                query = cache_vertex<COUNT, BATCH>(S, F, A, slot, path, pid, o, d, feat, w);
             } else {
-                float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
-                set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, depth);
+                Ray ray;
+                reset(ray, scale_add(d, kTraceOffset, o), d);
+                Hit hit;
+                int g = load_hit(A.hits, slot, hit);
+                float4 pc = A.depth == 1 ? make_float4(0, 0, 0, INFINITY) : A.path_color[path];
+                float3 color = xyz(pc), throughput = A.depth == 1 ? f3(1, 1, 1) : xyz(A.path_throughput[path]);
+                float depth = pc.w;
+                float3 current = f3(0, 0, 0), next_throughput = f3(0, 0, 0);
+                float hit_distance = INFINITY;
+                if (g >= 0) {
+                    hit_distance = hit.distance;
+                    Geo geo = load_geo(S, (uint32_t)g);
+                    Mat m = load_mat(S, geo.material);
+                    if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+                        current = m.emission;
+                    } else {
+                        Surface s;
+                        prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
+                        hit_distance = hit.distance;
+                        if (A.depth == 1) depth = depth_at(F.projection, hit.position);
+                        unsigned long long occluded = A.masks[slot];
+                        for (uint32_t i = 0; i < S.light_count; i++) {
+                            LightRec l = load_light(S, i);
+                            if (!is_facing_light(s, l)) continue;
+                            if ((l.flags & SLIM_LIGHT_IS_SHADOWING) && ((occluded >> i) & 1ull)) continue;
+                            add_light(s, m, l, current);
+                        }
+                        if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
+                        if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
+                            s.L = s.N;
+                            s.NdotL = 1.0f;
+                            float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
+                            float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
+                            radiance_fraction(s, m);
+                            current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
+                        }
+                        if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && A.depth < st.max_depth) {
+                            float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
+                            next_throughput = s.refracted ? one_minus(Fr) : Fr;
+                            bounce = true;
+                            bo = hit.position;
+                            bd = s.RF;
+                            reset(ray, bo, bd);
+                        }
+                    }
+                } else if (st.skybox_color_texture_id >= 0) {
+                    current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+                }
+                if (A.depth != A.skip_glow_depth) add_glow(S, ray, hit_distance, current);
+                color = mul_add(current, throughput, color);
+                throughput = throughput * next_throughput;
+                if (bounce) {
+                    A.path_color[path] = make_float4(color.x, color.y, color.z, depth);
+                    A.path_throughput[path] = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+                } else if (A.sink) {
+                    A.sink[path] = make_float4(color.x, color.y, color.z, 0.0f);
+                } else {
+                    write_pixel<BATCH>(F, pid, color, depth);
+                }
             }
         }
         uint32_t q = warp_append(A.count_out, bounce);
         if (bounce) {
             bump<COUNT>(w.bounce);
-            A.rays_out[2 * (size_t)q] = make_float4(bo.x, bo.y, bo.z, __uint_as_float(pixel));
-            A.rays_out[2 * (size_t)q + 1] = make_float4(bd.x, bd.y, bd.z, __uint_as_float(cone_pixel));
+            A.rays_out[2 * (size_t)q] = make_float4(bo.x, bo.y, bo.z, __uint_as_float(path));
+            A.rays_out[2 * (size_t)q + 1] = make_float4(bd.x, bd.y, bd.z, __uint_as_float(pid));
+        }
+        if (BATCH) {
+            uint32_t cq = warp_append(A.cache.count, query);
+            if (query) append_query(A.cache, cq, feat, o, d, path, pid);
         }
     }
     flush_stage<COUNT>(A.counters, w);
 }
 
 // ---- radiance cache ----------------------------------------------------------
-struct CacheArgs {
-    float4 *features, *aux, *radiance;
-    uint32_t *count;               // queries
-    uint32_t *train_count;         // training paths
-    uint32_t train_capacity;
-    float4 *t_features, *t_targets, *t_color, *t_through;
-    float offset;
-    int mode;
-};
-
-// Vertex-`depth` hits of the main paths.  Misses and emissive quads finish the
-// path exactly as k_shade does; every other hit becomes a cache query: the
-// segment's glow is added to the path colour now, the surface's features are
-// appended for the network, and the path waits in path_color /
-// path_throughput for the answer.
+// Single-request frames: the round at the cache depth runs this instead of
+// shadows and shading.
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, QueueArgs A, CacheArgs C) {
     uint32_t n = queue_size(A);
-    const SlimRayTracerSettings &st = F.settings;
     Work w = {};
-    // scene box -> [0,1]^3 (longest side), from the scene BVH root
-    float4 r0 = make_float4(0, 0, 0, 1), r1 = make_float4(1, 1, 0, 0);
-    if (S.scene_node_count) { r0 = S.scene_nodes[0]; r1 = S.scene_nodes[1]; }
-    const float3 bmin = f3(r0.x, r0.y, r0.z);
-    const float ext = fmaxf(fmaxf(r0.w - r0.x, r1.x - r0.y), r1.y - r0.z);
-    const float inv = ext > 0.0f ? 1.0f / ext : 1.0f;
     uint32_t stride = gridDim.x * blockDim.x;
     uint32_t rounds = (n + stride - 1) / stride;
     for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
         bool query = false;
-        uint32_t pixel = 0, cone_pixel = 0;
+        uint32_t path = 0, pid = 0;
         float3 o = f3(0, 0, 0), d = f3(0, 0, 0);
-        float4 f0 = make_float4(0, 0, 0, 0), f1 = f0, f2 = f0, f3v = f0;
+        float4 feat[4];
         if (slot < n) {
-            load_ray(F, A, slot, o, d, pixel, cone_pixel);
-            Ray ray;
-            reset(ray, scale_add(d, kTraceOffset, o), d);
-            Hit hit;
-            int g = load_hit(A.hits, slot, hit);
-            float4 pc = A.path_color[pixel];
-            float3 color = xyz(pc), throughput = xyz(A.path_throughput[pixel]);
-            float3 current = f3(0, 0, 0);
-            float hit_distance = INFINITY;
-            if (g >= 0) {
-                hit_distance = hit.distance;
-                Geo geo = load_geo(S, (uint32_t)g);
-                Mat m = load_mat(S, geo.material);
-                if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
-                    current = m.emission;
-                } else {
-                    Surface s;
-                    prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling(F, cone_pixel), s, w);
-                    hit_distance = hit.distance;
-                    query = true;
-                    float3 p = (s.P - bmin) * inv;
-                    float3 al = m.albedo * s.albedo_from_map;
-                    f0 = make_float4(p.x, p.y, p.z, m.roughness);
-                    f1 = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
-                    f2 = make_float4(s.N.x, s.N.y, s.N.z, 0.0f);
-                    f3v = make_float4(al.x, al.y, al.z, 0.0f);
-                }
-            } else if (st.skybox_color_texture_id >= 0) {
-                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
-            }
-            add_glow(S, ray, hit_distance, current);
-            color = mul_add(current, throughput, color);
-            if (query) {
-                A.path_color[pixel] = make_float4(color.x, color.y, color.z, pc.w);
-            } else {
-                float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
-                set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, pc.w);
-            }
+            load_ray(F, A, slot, o, d, path, pid);
+            query = cache_vertex<COUNT, false>(S, F, A, slot, path, pid, o, d, feat, w);
         }
         uint32_t q = warp_append(C.count, query);
-        if (query) {
-            float4 *f = C.features + 4 * (size_t)q;
-            f[0] = f0; f[1] = f1; f[2] = f2; f[3] = f3v;
-            C.aux[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __uint_as_float(pixel));
-            C.aux[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(cone_pixel));
-        }
+        if (query) append_query(C, q, feat, o, d, path, pid);
     }
     flush_stage<COUNT>(A.counters, w);
 }
@@ -609,14 +997,17 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
 // Training paths: query j of the frame's training set restarts from the
 // query's ray with zero colour and unit throughput in its own slot j.  With
 // more queries than training paths the set is stratified: j takes query
-// floor((j + offset) * queries / capacity).
+// floor((j + u) * queries / capacity), u = frac(0.618034 * frame) (a
+// golden-ratio sequence, so consecutive frames train on different queries).
 __global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
     const uint32_t nq = *C.count, cap = C.train_capacity;
     const uint32_t n = nq < cap ? nq : cap;
+    const double f = (double)*C.frame_counter * 0.6180339887498949;
+    const double u = f - floor(f);
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         uint32_t idx = j;
         if (nq > cap) {
-            idx = (uint32_t)(((double)j + (double)C.offset) * (double)nq / (double)cap);
+            idx = (uint32_t)(((double)j + u) * (double)nq / (double)cap);
             if (idx >= nq) idx = nq - 1;
         }
         if (C.t_features) {
@@ -638,19 +1029,270 @@ __global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
 
 // Waiting paths take the cache's answer: colour += throughput * radiance,
 // then tone mapping and the canvas write of k_shade.
-__global__ void k_cache_resolve(DevFrame F, CacheArgs C, const float4 *path_color, const float4 *path_throughput) {
+template <bool BATCH>
+__global__ void k_cache_resolve(DevFrame F0, QueueArgs A, const float4 *path_color, const float4 *path_throughput) {
+    const CacheArgs &C = A.cache;
     const uint32_t nq = *C.count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(C.frame_counter, 1u);
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
-        uint32_t pixel = __float_as_uint(C.aux[2 * (size_t)q].w);
-        float4 pc = path_color[pixel];
-        float3 thr = xyz(path_throughput[pixel]);
+        uint32_t path = __float_as_uint(C.aux[2 * (size_t)q].w);
+        uint32_t pid = __float_as_uint(C.aux[2 * (size_t)q + 1].w);
+        float4 pc = path_color[path];
+        float3 thr = xyz(path_throughput[path]);
         float3 L = f3(0, 0, 0);
         if (C.mode == SLIM_CACHE_ON) L = xyz(C.radiance[q]);
         else if (C.mode == SLIM_CACHE_EXACT) L = xyz(C.t_targets[q]);
-        float3 color = mul_add(L, thr, xyz(pc));
-        float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
-        set_pixel(F, (int)(pixel % F.width), (int)(pixel / F.width), c, pc.w);
+        write_pixel<BATCH>(frame_of<BATCH>(F0, A, pid), pid, mul_add(L, thr, xyz(pc)), pc.w);
     }
+}
+
+// ---- batched requests: primary rays of a wave --------------------------------
+// tiles[t] = (request, first pixel, pixel count, first slot), slots ascending.
+__global__ void k_batch_generate(QueueArgs A, const uint4 *__restrict__ tiles, uint32_t tile_count, float4 *rays,
+                                 uint32_t *ray_count, uint32_t wave_samples, unsigned long long *counters) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < wave_samples; s += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = tile_count;          // last tile with first slot <= s
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(&tiles[mid].w) <= s) lo = mid; else hi = mid;
+        }
+        uint4 t = tiles[lo];
+        uint32_t pixel = t.y + (s - t.w);
+        float3 o, d;
+        primary_ray(A.frames[t.x], pixel, o, d);
+        rays[2 * (size_t)s] = make_float4(o.x, o.y, o.z, __uint_as_float(s));
+        rays[2 * (size_t)s + 1] = make_float4(d.x, d.y, d.z, __uint_as_float((t.x << kBatchPixelBits) | pixel));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *ray_count = wave_samples;
+        if (counters) atomicAdd(counters, (unsigned long long)wave_samples);   // primary rays
+    }
+}
+
+// ---- frame orchestration ------------------------------------------------------
+struct RoundLaunch {
+    const DevScene *S;
+    const DevFrame *F;
+    const WavefrontBuffers *B;
+    int block, sms;
+    cudaStream_t stream;
+    StageTimer *timer;
+    unsigned long long *counters;
+    uint32_t bound;      // queue capacity (one ray per path slot)
+    uint32_t lights;     // most lights of any scene in the round
+    bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
+    unsigned long long *stage(int st) const { return counters ? counters + kCountersPerStage * st : nullptr; }
+    uint32_t grid(const void *kernel, uint32_t work) const {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+        uint32_t g = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
+        uint32_t need = (work + block - 1) / block;
+        return need < g ? (need ? need : 1) : g;
+    }
+};
+
+// One bounce round over the queue `in` (primary rays at depth 1 of a single
+// frame): extend, then shadows and shading -- or, at a single frame's cache
+// depth, the cache gather.  Leaves `in` at the round's output queue.
+template <bool COUNT, bool BATCH>
+cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA, uint32_t &in, uint32_t depth,
+                        bool primary, bool gather) {
+    const WavefrontBuffers &B = *L.B;
+    const DevScene &S = *L.S;
+    const DevFrame &F = *L.F;
+    cudaStream_t stream = L.stream;
+    StageTimer *timer = L.timer;
+    uint32_t out = in ^ 1u;
+    A.depth = depth;
+    A.rays_in = primary ? nullptr : B.rays[in];
+    A.count_in = primary ? nullptr : B.queue_count + in;
+    A.rays_out = B.rays[out];
+    A.count_out = B.queue_count + out;
+    // the output queue of this round is the input of the next: clear it
+    cudaError_t r = cudaMemsetAsync(B.queue_count + out, 0, sizeof(uint32_t), stream);
+    if (r != cudaSuccess) return r;
+    A.counters = L.stage(STAGE_EXTEND);
+    if (timer) timer->begin(STAGE_EXTEND, stream);
+    if (L.split_extend && B.pair_capacity >= 4) {
+        // [3] candidates, [4] candidate cursor, [5] overflowed rays
+        r = cudaMemsetAsync(B.queue_count + 3, 0, 3 * sizeof(uint32_t), stream);
+        if (r != cudaSuccess) return r;
+        k_extend_scene<COUNT, BATCH><<<L.grid((const void *)k_extend_scene<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        k_extend_mesh<COUNT><<<L.grid((const void *)k_extend_mesh<COUNT>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        k_extend_resolve<COUNT, BATCH><<<L.grid((const void *)k_extend_resolve<COUNT, BATCH>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        k_extend_overflow<COUNT, BATCH><<<L.grid((const void *)k_extend_overflow<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+    } else {
+        k_extend<COUNT, BATCH><<<L.grid((const void *)k_extend<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+    }
+    if (timer) timer->end(STAGE_EXTEND, stream);
+    if (gather) {
+        A.counters = L.stage(STAGE_CACHE);
+        if (timer) timer->begin(STAGE_CACHE, stream);
+        k_cache_gather<COUNT><<<L.grid((const void *)k_cache_gather<COUNT>, L.bound), L.block, 0, stream>>>(S, F, A, CA);
+        count_launch();
+        if (timer) timer->end(STAGE_CACHE, stream);
+        in = out;
+        return cudaGetLastError();
+    }
+    // Shadow rays in light batches that fit the shadow queue.
+    uint32_t per_batch = B.shadow_capacity / (L.bound ? L.bound : 1);
+    if (per_batch < 1) per_batch = 1;
+    for (uint32_t l0 = 0; l0 < L.lights; l0 += per_batch) {
+        A.light_begin = l0;
+        A.light_end = l0 + per_batch < L.lights ? l0 + per_batch : L.lights;
+        r = cudaMemsetAsync(B.queue_count + 2, 0, sizeof(uint32_t), stream);
+        if (r != cudaSuccess) return r;
+        A.shadow_count = B.queue_count + 2;
+        A.counters = L.stage(STAGE_SHADOW_GEN);
+        if (timer) timer->begin(STAGE_SHADOW_GEN, stream);
+        k_shadow_gen<COUNT, BATCH><<<L.grid((const void *)k_shadow_gen<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        if (timer) timer->end(STAGE_SHADOW_GEN, stream);
+        r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
+        if (r != cudaSuccess) return r;
+        A.counters = L.stage(STAGE_SHADOW);
+        if (timer) timer->begin(STAGE_SHADOW, stream);
+        k_shadow_scene<COUNT, BATCH><<<L.grid((const void *)k_shadow_scene<COUNT, BATCH>, L.bound * (A.light_end - A.light_begin)),
+                                      L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        if (timer) timer->end(STAGE_SHADOW, stream);
+        A.counters = L.stage(STAGE_SHADOW_MESH);
+        if (timer) timer->begin(STAGE_SHADOW_MESH, stream);
+        k_shadow_mesh<COUNT><<<L.grid((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        if (timer) timer->end(STAGE_SHADOW_MESH, stream);
+    }
+    A.counters = L.stage(STAGE_SHADE);
+    if (timer) timer->begin(STAGE_SHADE, stream);
+    k_shade<COUNT, BATCH><<<L.grid((const void *)k_shade<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
+    count_launch();
+    if (timer) timer->end(STAGE_SHADE, stream);
+    in = out;
+    return cudaGetLastError();
+}
+
+CacheArgs cache_args(const CacheFrame *cache) {
+    CacheArgs CA{};
+    if (!cache) return CA;
+    CA.features = cache->features;
+    CA.aux = cache->aux;
+    CA.radiance = cache->radiance;
+    CA.count = cache->counts;
+    CA.train_count = cache->counts + 1;
+    CA.train_capacity = cache->train_capacity;
+    CA.t_features = cache->mode == SLIM_CACHE_ON ? cache->t_features : nullptr;
+    CA.t_targets = cache->t_targets;
+    CA.t_color = cache->t_color;
+    CA.t_through = cache->t_through;
+    CA.frame_counter = cache->frame_counter;
+    CA.mode = cache->mode;
+    return CA;
+}
+
+// After the queries of a frame (or wave) are gathered: the training paths
+// traced on to max_depth, the Adam steps, the network's answers, and the
+// waiting paths resolved.
+template <bool COUNT, bool BATCH>
+cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA, uint32_t &in, const CacheFrame *cache,
+                        uint32_t max_depth) {
+    const WavefrontBuffers &B = *L.B;
+    cudaStream_t stream = L.stream;
+    StageTimer *timer = L.timer;
+    cudaError_t e;
+    const int mode = cache->mode;
+    const bool train = mode == SLIM_CACHE_ON && cache->trainer && cache->batch && cache->train_capacity;
+    if (train && cache->train_stream && cache->train_queues && !BATCH) {
+        // Overlapped training.  The previous frame's training has finished
+        // once `trained` completes: take its weights for this frame's
+        // queries, then hand this frame's training paths to the training
+        // stream, which traces them with its own queues while this stream
+        // answers the queries and the next frame's primary rays run.
+        const WavefrontBuffers &TB = *cache->train_queues;
+        cudaStream_t ts = cache->train_stream;
+        if ((e = cudaStreamWaitEvent(stream, cache->trained, 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync((void *)cache->weights, cache->train_weights, nrc::kImgBytes, cudaMemcpyDeviceToDevice,
+                                 stream)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(TB.queue_count, 0, 8 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
+        if (timer) timer->begin(STAGE_CACHE, stream);
+        uint32_t g = (cache->train_capacity + 255) / 256;
+        if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, TB.rays[0], TB.queue_count);
+        count_launch();
+        if (timer) timer->end(STAGE_CACHE, stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(cache->selected, stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(ts, cache->selected, 0)) != cudaSuccess) return e;
+        RoundLaunch TL{L.S, L.F, &TB, L.block, L.sms, ts, nullptr, nullptr, TB.capacity, L.lights, L.split_extend};
+        QueueArgs TA = A;
+        TA.hits = TB.hits;
+        TA.shadow_rays = TB.shadow_rays;
+        TA.masks = TB.shadow_mask;
+        TA.pairs = TB.pairs;
+        TA.pair_count = TB.queue_count + 3;
+        TA.pair_cursor = TB.queue_count + 4;
+        TA.pair_capacity = TB.pair_capacity;
+        TA.path_color = cache->t_color;
+        TA.path_throughput = cache->t_through;
+        TA.sink = cache->t_targets;
+        TA.skip_glow_depth = cache->depth;
+        TA.samples = TB.capacity;
+        uint32_t tin = 0;
+        for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
+            if ((e = trace_round<false, false>(TL, TA, CA, tin, depth, false, false)) != cudaSuccess) return e;
+        for (uint32_t off = 0; off < cache->train_capacity; off += cache->batch) {
+            uint32_t n = cache->train_capacity - off < cache->batch ? cache->train_capacity - off : cache->batch;
+            if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, ts)) !=
+                cudaSuccess)
+                return e;
+        }
+        if ((e = cudaEventRecord(cache->trained, ts)) != cudaSuccess) return e;
+    } else if (mode == SLIM_CACHE_EXACT || train) {
+        if (timer) timer->begin(STAGE_CACHE, stream);
+        uint32_t g = (cache->train_capacity + 255) / 256;
+        if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in);
+        count_launch();
+        if (timer) timer->end(STAGE_CACHE, stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        QueueArgs main = A;
+        A.path_color = cache->t_color;
+        A.path_throughput = cache->t_through;
+        A.sink = cache->t_targets;
+        A.skip_glow_depth = cache->depth;
+        for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
+            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+        A = main;
+    }
+    if (train && !(cache->train_stream && cache->train_queues && !BATCH)) {
+        if (timer) timer->begin(STAGE_CACHE_TRAIN, stream);
+        for (uint32_t off = 0; off < cache->train_capacity; off += cache->batch) {
+            uint32_t n = cache->train_capacity - off < cache->batch ? cache->train_capacity - off : cache->batch;
+            if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, stream)) !=
+                cudaSuccess)
+                return e;
+        }
+        if (timer) timer->end(STAGE_CACHE_TRAIN, stream);
+    }
+    if (mode == SLIM_CACHE_ON) {
+        if (timer) timer->begin(STAGE_CACHE_QUERY, stream);
+        e = nrc::launch_infer(cache->features, cache->counts, 0, L.bound, cache->radiance, cache->weights,
+                              L.F->error_flags, stream);
+        if (timer) timer->end(STAGE_CACHE_QUERY, stream);
+        if (e != cudaSuccess) return e;
+    }
+    if (timer) timer->begin(STAGE_CACHE, stream);
+    A.cache = CA;
+    k_cache_resolve<BATCH><<<L.grid((const void *)k_cache_resolve<BATCH>, L.bound), L.block, 0, stream>>>(
+        *L.F, A, B.path_color, B.path_throughput);
+    count_launch();
+    if (timer) timer->end(STAGE_CACHE, stream);
+    return cudaGetLastError();
 }
 
 template <bool COUNT>
@@ -660,19 +1302,8 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (block <= 0) block = 256;
-    // Persistent-style grids: enough resident blocks to fill every SM, the
-    // threads stride over the device-side queue length.
-    auto grid_for = [&](const void *kernel, uint32_t work) {
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
-        uint32_t g = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
-        uint32_t need = (work + block - 1) / block;
-        return need < g ? (need ? need : 1) : g;
-    };
-    uint32_t lights = S.light_count;
-    unsigned long long *C = F.counters;
-    auto stage_counters = [&](int stage) { return C ? C + kCountersPerStage * stage : nullptr; };
+    RoundLaunch L{&S, &F, &B, block <= 0 ? 256 : block, sms, stream, timer, F.counters, samples, S.light_count,
+                  S.mesh_count > 0};
     cudaError_t e = cudaMemsetAsync(B.queue_count, 0, 8 * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     QueueArgs A{};
@@ -688,130 +1319,67 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     A.samples = samples;
     const uint32_t max_depth = F.settings.max_depth;
     const bool use_cache = cache && cache->mode != SLIM_CACHE_OFF && cache->depth >= 2 && cache->depth <= max_depth;
-    CacheArgs CA{};
-    if (use_cache) {
-        CA.features = cache->features;
-        CA.aux = cache->aux;
-        CA.radiance = cache->radiance;
-        CA.count = cache->counts;
-        CA.train_count = cache->counts + 1;
-        CA.train_capacity = cache->train_capacity;
-        CA.t_features = cache->mode == SLIM_CACHE_ON ? cache->t_features : nullptr;
-        CA.t_targets = cache->t_targets;
-        CA.t_color = cache->t_color;
-        CA.t_through = cache->t_through;
-        CA.offset = cache->select_offset;
-        CA.mode = cache->mode;
-        e = cudaMemsetAsync(cache->counts, 0, 2 * sizeof(uint32_t), stream);
-        if (e != cudaSuccess) return e;
-    }
-    const uint32_t bound = samples;   // a queue holds at most one ray per sample
-
-    // One bounce round over the queue `in` (primary rays at depth 1): extend,
-    // then shadows and shading -- or, at the cache depth, the cache gather.
+    CacheArgs CA = use_cache ? cache_args(cache) : CacheArgs{};
+    // Only the query count starts over: the training count belongs to the
+    // training set, which the overlapped training stream may still be using;
+    // the selection that replaces the set rewrites it.
+    if (use_cache && (e = cudaMemsetAsync(cache->counts, 0, sizeof(uint32_t), stream)) != cudaSuccess) return e;
     uint32_t in = 0;
-    auto round = [&](uint32_t depth, bool primary, bool gather) -> cudaError_t {
-        uint32_t out = in ^ 1u;
-        A.depth = depth;
-        A.rays_in = primary ? nullptr : B.rays[in];
-        A.count_in = primary ? nullptr : B.queue_count + in;
-        A.rays_out = B.rays[out];
-        A.count_out = B.queue_count + out;
-        // the output queue of this round is the input of the next: clear it
-        if (!primary) {
-            cudaError_t r = cudaMemsetAsync(B.queue_count + out, 0, sizeof(uint32_t), stream);
-            if (r != cudaSuccess) return r;
-        }
-        A.counters = stage_counters(STAGE_EXTEND);
-        if (timer) timer->begin(STAGE_EXTEND, stream);
-        k_extend<COUNT><<<grid_for((const void *)k_extend<COUNT>, bound), block, 0, stream>>>(S, F, A);
-        if (timer) timer->end(STAGE_EXTEND, stream);
-        if (gather) {
-            A.counters = stage_counters(STAGE_CACHE);
-            if (timer) timer->begin(STAGE_CACHE, stream);
-            k_cache_gather<COUNT><<<grid_for((const void *)k_cache_gather<COUNT>, bound), block, 0, stream>>>(S, F, A, CA);
-            if (timer) timer->end(STAGE_CACHE, stream);
-            in = out;
-            return cudaGetLastError();
-        }
-        // Shadow rays in light batches that fit the shadow queue.
-        uint32_t per_batch = B.shadow_capacity / (samples ? samples : 1);
-        if (per_batch < 1) per_batch = 1;
-        for (uint32_t l0 = 0; l0 < lights; l0 += per_batch) {
-            A.light_begin = l0;
-            A.light_end = l0 + per_batch < lights ? l0 + per_batch : lights;
-            cudaError_t r = cudaMemsetAsync(B.queue_count + 2, 0, sizeof(uint32_t), stream);
-            if (r != cudaSuccess) return r;
-            A.shadow_count = B.queue_count + 2;
-            A.counters = stage_counters(STAGE_SHADOW_GEN);
-            if (timer) timer->begin(STAGE_SHADOW_GEN, stream);
-            k_shadow_gen<COUNT><<<grid_for((const void *)k_shadow_gen<COUNT>, bound), block, 0, stream>>>(S, F, A);
-            if (timer) timer->end(STAGE_SHADOW_GEN, stream);
-            r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
-            if (r != cudaSuccess) return r;
-            A.counters = stage_counters(STAGE_SHADOW);
-            if (timer) timer->begin(STAGE_SHADOW, stream);
-            k_shadow_scene<COUNT><<<grid_for((const void *)k_shadow_scene<COUNT>, bound * (A.light_end - A.light_begin)), block, 0, stream>>>(S, F, A);
-            if (timer) timer->end(STAGE_SHADOW, stream);
-            A.counters = stage_counters(STAGE_SHADOW_MESH);
-            if (timer) timer->begin(STAGE_SHADOW_MESH, stream);
-            k_shadow_mesh<COUNT><<<grid_for((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), block, 0, stream>>>(S, F, A);
-            if (timer) timer->end(STAGE_SHADOW_MESH, stream);
-        }
-        A.counters = stage_counters(STAGE_SHADE);
-        if (timer) timer->begin(STAGE_SHADE, stream);
-        k_shade<COUNT><<<grid_for((const void *)k_shade<COUNT>, bound), block, 0, stream>>>(S, F, A);
-        if (timer) timer->end(STAGE_SHADE, stream);
-        in = out;
-        return cudaGetLastError();
-    };
-
     const uint32_t last = use_cache ? cache->depth : max_depth;
     for (uint32_t depth = 1; depth <= last; depth++)
-        if ((e = round(depth, depth == 1, use_cache && depth == last)) != cudaSuccess) return e;
+        if ((e = trace_round<COUNT, false>(L, A, CA, in, depth, depth == 1, use_cache && depth == last)) != cudaSuccess)
+            return e;
     if (!use_cache) return cudaSuccess;
+    A.cache = CA;
+    return cache_phase<COUNT, false>(L, A, CA, in, cache, max_depth);
+}
 
-    const int mode = cache->mode;
-    const bool train = mode == SLIM_CACHE_ON && cache->trainer && cache->batch && cache->train_capacity;
-    if (mode == SLIM_CACHE_EXACT || train) {
-        // training paths continue from the cache vertex in their own slots
-        if (timer) timer->begin(STAGE_CACHE, stream);
-        uint32_t g = (cache->train_capacity + 255) / 256;
+// Batched requests: every wave is a full multi-request frame over its slots.
+template <bool COUNT>
+cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
+                      StageTimer *timer) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const CacheFrame *cache = BF.cache;
+    CacheArgs CA = cache_args(cache);
+    cudaError_t e;
+    for (uint32_t wi = 0; wi < BF.wave_count; wi++) {
+        const BatchWave &wave = BF.waves[wi];
+        RoundLaunch L{&BF.shared, &BF.frame, &B, block <= 0 ? 256 : block, sms, stream, timer, BF.frame.counters,
+                      B.capacity, wave.max_lights, BF.shared.mesh_count > 0};
+        if ((e = cudaMemsetAsync(B.queue_count, 0, 8 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
+        const bool use_cache = cache && wave.cache_paths;
+        if (use_cache && (e = cudaMemsetAsync(cache->counts, 0, sizeof(uint32_t), stream)) != cudaSuccess)
+            return e;
+        QueueArgs A{};
+        A.hits = B.hits;
+        A.shadow_rays = B.shadow_rays;
+        A.masks = B.shadow_mask;
+        A.pairs = B.pairs;
+        A.pair_count = B.queue_count + 3;
+        A.pair_cursor = B.queue_count + 4;
+        A.pair_capacity = B.pair_capacity;
+        A.path_color = B.path_color;
+        A.path_throughput = B.path_throughput;
+        A.samples = wave.samples;
+        A.scenes = BF.scenes;
+        A.frames = BF.frames;
+        A.cache = CA;
+        if (timer) timer->begin(STAGE_EXTEND, stream);
+        uint32_t g = (wave.samples + 255) / 256;
         if (g > (uint32_t)(sms * 8)) g = (uint32_t)(sms * 8);
-        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in);
-        if (timer) timer->end(STAGE_CACHE, stream);
+        k_batch_generate<<<g ? g : 1, 256, 0, stream>>>(A, BF.tiles + wave.first_tile, wave.tile_count, B.rays[0],
+                                                         B.queue_count, wave.samples, L.stage(STAGE_EXTEND));
+        count_launch();
+        if (timer) timer->end(STAGE_EXTEND, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        QueueArgs main = A;
-        A.path_color = cache->t_color;
-        A.path_throughput = cache->t_through;
-        A.sink = cache->t_targets;
-        A.skip_glow_depth = cache->depth;
-        for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
-            if ((e = round(depth, false, false)) != cudaSuccess) return e;
-        A = main;
+        uint32_t in = 0;
+        for (uint32_t depth = 1; depth <= wave.max_depth; depth++)
+            if ((e = trace_round<COUNT, true>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+        if (use_cache && (e = cache_phase<COUNT, true>(L, A, CA, in, cache, wave.max_depth)) != cudaSuccess) return e;
     }
-    if (train) {
-        if (timer) timer->begin(STAGE_CACHE_TRAIN, stream);
-        for (uint32_t off = 0; off < cache->train_capacity; off += cache->batch) {
-            uint32_t n = cache->train_capacity - off < cache->batch ? cache->train_capacity - off : cache->batch;
-            if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, stream)) !=
-                cudaSuccess)
-                return e;
-        }
-        if (timer) timer->end(STAGE_CACHE_TRAIN, stream);
-    }
-    if (mode == SLIM_CACHE_ON) {
-        if (timer) timer->begin(STAGE_CACHE_QUERY, stream);
-        e = nrc::launch_infer(cache->features, cache->counts, 0, samples, cache->radiance, cache->weights,
-                              F.error_flags, stream);
-        if (timer) timer->end(STAGE_CACHE_QUERY, stream);
-        if (e != cudaSuccess) return e;
-    }
-    if (timer) timer->begin(STAGE_CACHE, stream);
-    k_cache_resolve<<<grid_for((const void *)k_cache_resolve, bound), block, 0, stream>>>(F, CA, B.path_color,
-                                                                                          B.path_throughput);
-    if (timer) timer->end(STAGE_CACHE, stream);
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 }  // namespace dev
@@ -823,6 +1391,12 @@ cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const 
     if (F.settings.max_depth == 0) return launch_render_fused(S, F, block, stream, timer);
     if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer, cache);
     return dev::run_frame<false>(S, F, B, block, stream, timer, cache);
+}
+
+cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
+                                StageTimer *timer) {
+    if (BF.frame.counters) return dev::run_batch<true>(BF, B, block, stream, timer);
+    return dev::run_batch<false>(BF, B, block, stream, timer);
 }
 
 }  // namespace slim

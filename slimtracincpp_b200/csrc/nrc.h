@@ -12,6 +12,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "launch_count.h"
 
 namespace slim {
 namespace nrc {
@@ -33,9 +34,14 @@ constexpr uint32_t kErrTimeout = 4u;
 
 struct AdamArgs {
     float lr, beta1, beta2, eps;
-    float bias1, bias2;      // 1 / (1 - beta^step)
+    uint32_t *step;          // device step counter: the training kernel counts a non-empty
+                             // step, Adam reads it for the bias corrections (so a captured
+                             // graph replays correctly)
     uint32_t parts;          // partial gradient rows to sum (set by the launcher)
 };
+
+// Sets the kernels' shared-memory limits (before any launch or graph capture).
+cudaError_t prepare();
 
 // Largest grid the training kernel uses (rows of the partial-gradient buffer).
 int train_grid(uint32_t samples);

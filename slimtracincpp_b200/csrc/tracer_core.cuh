@@ -358,6 +358,32 @@ SLIM_D bool hit_triangles(const float4 *hot, uint32_t first, uint32_t count, flo
     return found;
 }
 
+// The attributes MeshTracer::trace fills in for a closest hit (mesh_tracer.h:
+// 116-133): the triangle's uv coverage and, with vertex normals / uvs, their
+// barycentric blend.  h.id is the triangle's leaf-order index in the mesh.
+template <bool COUNT>
+SLIM_D void mesh_hit_attributes(const DevScene &S, const DevMesh &m, Hit &h, Work &w) {
+    const float4 *c = S.tri_cold + 4 * (size_t)(m.tri_offset + h.id);
+    float4 c3 = __ldg(c + 3);
+    h.uv_coverage = c3.w;
+    if (m.has_normals | m.has_uvs) {
+        bump<COUNT>(w.mesh_fetches);
+        float4 c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2);
+        float A = h.u, B = h.v, C = 1 - A - B;
+        if (m.has_uvs) {
+            // uv1 = (c2.y, c2.z), uv2 = (c2.w, c3.x), uv3 = (c3.y, c3.z)
+            h.u = fmaf(c3.y, A, fmaf(c2.w, B, c2.y * C));
+            h.v = fmaf(c3.z, A, fmaf(c3.x, B, c2.z * C));
+        }
+        if (m.has_normals) {
+            // n1 = (c0.x, c0.y, c0.z), n2 = (c0.w, c1.x, c1.y), n3 = (c1.z, c1.w, c2.x)
+            h.normal.x = fmaf(c1.z, A, fmaf(c0.w, B, c0.x * C));
+            h.normal.y = fmaf(c1.w, A, fmaf(c1.x, B, c0.y * C));
+            h.normal.z = fmaf(c2.x, A, fmaf(c1.y, B, c0.z * C));
+        }
+    }
+}
+
 // MeshTracer::trace (mesh_tracer.h:51-134).  `stack` holds kStackCapacity
 // entries; overflow sets kErrStack and ends the traversal.
 template <bool COUNT>
@@ -424,25 +450,7 @@ SLIM_D bool mesh_trace(const DevScene &S, const DevMesh &m, const Ray &r, Hit &h
         }
     }
     if (found && !any_hit) {
-        const float4 *c = S.tri_cold + 4 * (size_t)(m.tri_offset + h.id);
-        float4 c3 = __ldg(c + 3);
-        h.uv_coverage = c3.w;
-        if (m.has_normals | m.has_uvs) {
-            bump<COUNT>(w.mesh_fetches);
-            float4 c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2);
-            float A = h.u, B = h.v, C = 1 - A - B;
-            if (m.has_uvs) {
-                // uv1 = (c2.y, c2.z), uv2 = (c2.w, c3.x), uv3 = (c3.y, c3.z)
-                h.u = fmaf(c3.y, A, fmaf(c2.w, B, c2.y * C));
-                h.v = fmaf(c3.z, A, fmaf(c3.x, B, c2.z * C));
-            }
-            if (m.has_normals) {
-                // n1 = (c0.x, c0.y, c0.z), n2 = (c0.w, c1.x, c1.y), n3 = (c1.z, c1.w, c2.x)
-                h.normal.x = fmaf(c1.z, A, fmaf(c0.w, B, c0.x * C));
-                h.normal.y = fmaf(c1.w, A, fmaf(c1.x, B, c0.y * C));
-                h.normal.z = fmaf(c2.x, A, fmaf(c1.y, B, c0.z * C));
-            }
-        }
+        mesh_hit_attributes<COUNT>(S, m, h, w);
     } else if (found) {
         h.uv_coverage = __ldg(&S.tri_cold[4 * (size_t)(m.tri_offset + h.id) + 3].w);
     }

@@ -92,10 +92,15 @@ RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4,
                       ("radiance_cache", i4, 28)], 32)
 CACHE_CONFIG = _dt([("cache_depth", u4, 0), ("train_samples", u4, 4), ("batch", u4, 8), ("seed", u4, 12),
                     ("learning_rate", f4, 16), ("beta1", f4, 20), ("beta2", f4, 24), ("epsilon", f4, 28),
-                    ("train", u4, 32), ("_reserved", (u4, 3), 36)], 48)
+                    ("train", u4, 32), ("overlap", u4, 36), ("_reserved", (u4, 2), 40)], 48)
 CACHE_STATS = _dt([("frames", u8, 0), ("steps", u8, 8), ("queries", u4, 16), ("train_samples", u4, 20),
                    ("loss", f4, 24), ("_pad", f4, 28)], 32)
 CACHE_OFF, CACHE_ON, CACHE_TRUNCATE, CACHE_EXACT = 0, 1, 2, 3
+RENDER_REQUEST = _dt([("scene", u8, 0), ("projection", PROJECTION, 8), ("settings", SETTINGS, 108),
+                      ("width", u4, 152), ("height", u4, 156), ("radiance_cache", i4, 160), ("_pad", u4, 164),
+                      ("d_pixels", u8, 168), ("d_depths", u8, 176)], 184)
+BATCH_PLAN = _dt([("queue_capacity", u4, 0), ("tile_pixels", u4, 4), ("block_size", i4, 8), ("waves", u4, 12),
+                  ("batch_ms", f4, 16), ("candidates", u4, 20), ("graph_nodes", u4, 24), ("tuned", u4, 28)], 32)
 NRC_PARAMS = 18624
 NRC_FEATURES = 16
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(

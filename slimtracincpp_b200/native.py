@@ -28,7 +28,9 @@ EXPORTS = [
     "slimGetStageStats", "slimResetStageStats", "slimRenderToDeviceNoAlloc",
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
-    "slimRadianceCacheTrain", "slimRadianceCacheGetStats",
+    "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimSynchronize",
+    "slimGetLaunchCount",
+    "slimBatchSetRequests", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender",
 ]
 
 
@@ -79,6 +81,9 @@ def lib():
     for name in ["slimRadianceCacheSetWeights", "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients"]:
         getattr(h, name).argtypes = [P, C.c_uint32]
     h.slimRadianceCacheQuery.argtypes = [P, C.c_uint32, P, P]
+    for name in ["slimSynchronize", "slimRadianceCacheJoin", "slimGetLaunchCount", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender"]:
+        getattr(h, name).argtypes = [P]
+    h.slimBatchSetRequests.argtypes = [P, C.c_uint32]
     h.slimRadianceCacheTrain.argtypes = [P, P, C.c_uint32, P]
     for name in EXPORTS:
         if name not in ("slimGetLastError",):
@@ -143,3 +148,10 @@ def work_counters():
     w = np.zeros((), L.WORK_COUNTERS)
     check(lib().slimGetWorkCounters(ptr(w)))
     return {k: int(w[k]) for k in L.WORK_COUNTERS.names}
+
+
+def launch_count():
+    """Kernels the library has launched since it was loaded."""
+    n = np.zeros(1, np.uint64)
+    check(lib().slimGetLaunchCount(ptr(n)))
+    return int(n[0])

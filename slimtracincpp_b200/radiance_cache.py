@@ -19,11 +19,11 @@ from .native import check, lib, ptr
 class RadianceCache:
     @staticmethod
     def configure(cache_depth=2, train_samples=65536, batch=16384, seed=0, learning_rate=1e-2, beta1=0.9,
-                  beta2=0.99, epsilon=1e-8, train=True):
+                  beta2=0.99, epsilon=1e-8, train=True, overlap=True):
         c = np.zeros((), L.CACHE_CONFIG)
         c["cache_depth"], c["train_samples"], c["batch"], c["seed"] = cache_depth, train_samples, batch, seed
         c["learning_rate"], c["beta1"], c["beta2"], c["epsilon"] = learning_rate, beta1, beta2, epsilon
-        c["train"] = int(bool(train))
+        c["train"], c["overlap"] = int(bool(train)), int(bool(overlap))
         check(lib().slimRadianceCacheConfigure(ptr(c)))
         return RadianceCache()
 
@@ -53,6 +53,10 @@ class RadianceCache:
 
     def train(self, d_features, d_targets, count, stream=0):
         check(lib().slimRadianceCacheTrain(int(d_features), int(d_targets), int(count), int(stream)))
+
+    def join(self, stream=0):
+        """Make `stream` wait for the overlapped training."""
+        check(lib().slimRadianceCacheJoin(int(stream)))
 
     def stats(self):
         s = np.zeros((), L.CACHE_STATS)

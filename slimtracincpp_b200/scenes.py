@@ -448,3 +448,88 @@ def config4(seed=0, width=1920, height=1080, meshes=None):
 
 
 CONFIGS = {"config1": config1, "config2": config2, "config3": config3, "config4": config4}
+
+
+# ---- config 5: batched requests ------------------------------------------------
+BATCH_RESOLUTIONS = [(320, 180), (640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+class Request:
+    """One render request of a batch: its own scene (mesh ids refer to the
+    shared assets), camera, canvas size, bounce depth and cache use."""
+
+    def __init__(self, name, scene, camera, width, height, settings, radiance_cache):
+        self.name, self.scene, self.camera = name, scene, camera
+        self.width, self.height, self.settings, self.radiance_cache = width, height, settings, radiance_cache
+
+    @property
+    def samples(self):
+        return self.width * self.height
+
+    def projection(self):
+        return self.camera.projection(self.width, self.height, False)
+
+    def workload(self):
+        return Workload(self.name, self.scene, self.camera, self.width, self.height, self.settings)
+
+
+def batch_request(rng, meshes, width, height, max_depth, radiance_cache, index=0):
+    """A seeded scene of 1-16 instances of the shared meshes and 0-8 implicit
+    primitives on a floor, with Cook-Torrance, glass and mirror materials
+    and 2-4 point lights."""
+    pbr = []
+    for _ in range(4):
+        metallic = int(rng.integers(0, 2))
+        m = L.default_material(albedo=0, roughness=float(rng.uniform(0.05, 1.0)), brdf=L.BRDF_COOK_TORRANCE,
+                               reflectivity=0.04, metalness=float(metallic),
+                               flags=L.MATERIAL_IS_REFLECTIVE if metallic else 0)
+        m["albedo"] = rng.uniform(0.2, 1.0, 3).astype(np.float32)
+        pbr.append(m)
+    glass = L.default_material(albedo=0.05, roughness=0.25, flags=L.MATERIAL_IS_REFRACTIVE, ior=1.5, reflectivity=0.04)
+    mirror = L.default_material(albedo=0.0, roughness=0.02, flags=L.MATERIAL_IS_REFLECTIVE,
+                                reflectivity=(0.91, 0.92, 0.92))
+    floor = L.default_material(albedo=0.8, roughness=0.8, brdf=L.BRDF_LAMBERT)
+    materials = [floor] + pbr + [glass, mirror]
+    GLASS, MIRROR = 5, 6
+    geos = [geometry(L.GEOMETRY_QUAD, 0, (0, 0, 0), (12, 1, 12))]
+    for _ in range(int(rng.integers(1, 17))):
+        axis, amount = random_quat(rng)
+        s = np.float32(rng.uniform(0.5, 2.0))
+        pos = (rng.uniform(-7, 7), rng.uniform(0.5, 3.0), rng.uniform(-4, 8))
+        r = rng.uniform()
+        mid = GLASS if r < 0.15 else MIRROR if r < 0.3 else int(rng.integers(1, 5))
+        flags = L.GEOMETRY_IS_VISIBLE if mid == GLASS else L.GEOMETRY_IS_VISIBLE | L.GEOMETRY_IS_SHADOWING
+        geos.append(geometry(L.GEOMETRY_MESH, mid, pos, (s, s, s), axis, amount, mesh_id=int(rng.integers(0, len(meshes))),
+                             flags=flags))
+    kinds = [L.GEOMETRY_SPHERE, L.GEOMETRY_BOX, L.GEOMETRY_TET, L.GEOMETRY_QUAD]
+    for _ in range(int(rng.integers(0, 9))):
+        kind = kinds[int(rng.integers(0, 4))]
+        r = rng.uniform()
+        mid = GLASS if (r < 0.25 and kind == L.GEOMETRY_SPHERE) else MIRROR if r < 0.4 else int(rng.integers(1, 5))
+        flags = L.GEOMETRY_IS_VISIBLE if mid == GLASS else L.GEOMETRY_IS_VISIBLE | L.GEOMETRY_IS_SHADOWING
+        s = np.float32(rng.uniform(0.5, 1.5))
+        x, z = rng.uniform(-6, 6), rng.uniform(-4, 8)
+        axis, amount = quat_y(rng.uniform(0, 2 * np.pi))
+        y = s if kind != L.GEOMETRY_TET else np.float32(s * TET_MAX)
+        geos.append(geometry(kind, mid, (x, y, z), (s, s, s), axis, amount, flags=flags))
+    lights = [light(rng.uniform(0.6, 1.0, 3), (rng.uniform(-8, 8), rng.uniform(4, 8), rng.uniform(-8, 4)),
+                    rng.uniform(15, 50)) for _ in range(int(rng.integers(2, 5)))]
+    scene = Scene(np.array(geos), np.array(materials), np.array(lights), meshes=meshes)
+    eye = (rng.uniform(-3, 3), rng.uniform(4, 7), rng.uniform(-15, -11))
+    cam = Camera.look_at(eye, (0.0, 1.0, 2.0), 60.0)
+    return Request(f"request{index}_{width}x{height}_d{max_depth}{'_cache' if radiance_cache else ''}", scene, cam,
+                   width, height, L.default_settings(max_depth=max_depth), radiance_cache)
+
+
+def config5(seed=0, count=64, meshes=None, resolutions=None):
+    """64 requests: resolutions drawn uniformly from 320x180 ... 3840x2160,
+    bounce depth 1-8, every other request with the radiance cache."""
+    rng = np.random.default_rng(seed)
+    meshes = meshes if meshes is not None else config2_meshes()
+    resolutions = resolutions or BATCH_RESOLUTIONS
+    out = []
+    for i in range(count):
+        w, h = resolutions[int(rng.integers(0, len(resolutions)))]
+        depth = int(rng.integers(1, 9))
+        out.append(batch_request(rng, meshes, w, h, depth, L.CACHE_ON if i % 2 == 0 else L.CACHE_OFF, i))
+    return out

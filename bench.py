@@ -65,6 +65,23 @@ def dist_info():
     return rank, world, local
 
 
+def max_over_ranks(values, device, world):
+    """Every rank's timings reduced to the slowest rank's (the job ends when
+    the last replica does): an all-reduce MAX over the process group."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def whole_job_rate(units_per_rank_step, steps, world, total_ms):
+    """Units all ranks processed per second (replicas: every rank does the
+    same per-step work), in millions."""
+    return units_per_rank_step * steps * world / (total_ms / 1000.0) / 1e6
+
+
 def device_uuid(dev):
     """NVML name of the CUDA device (CUDA_VISIBLE_DEVICES may renumber devices)."""
     try:
@@ -395,11 +412,8 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     e2e_s = time.perf_counter() - t0
     native.set_render_options(engine=L.ENGINE_WAVEFRONT)
 
-    times = torch.tensor([sum(cache_ms), sum(plain_ms), e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    cache_total, plain_total, e2e_s = float(times[0]), float(times[1]), float(times[2])
-    value = cache_rays * steps * world / (cache_total / 1000.0) / 1e6
+    cache_total, plain_total, e2e_s = max_over_ranks([sum(cache_ms), sum(plain_ms), e2e_s], dev, world)
+    value = whole_job_rate(cache_rays, steps, world, cache_total)
     timed = {k: v for k, v in stats.items() if v["launches"]}
     stages = {k: v["total_ms"] / steps for k, v in timed.items()}
     q = stats.get("cache_query")
@@ -527,12 +541,9 @@ def run_batch_bench(args, torch, dist, dev, rank, world, local):
         torch.cuda.synchronize()
         single_ms.append(a.elapsed_time(b) / 3)
 
-    times = torch.tensor([sum(batch_ms), e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_s = float(times[0]), float(times[1])
+    total_ms, e2e_s = max_over_ranks([sum(batch_ms), e2e_s], dev, world)
     ms = total_ms / args.steps
-    value = rays * args.steps * world / (total_ms / 1000.0) / 1e6
+    value = whole_job_rate(rays, args.steps, world, total_ms)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 trace, bf16 MLP (f32 accumulate)",
@@ -669,12 +680,9 @@ def main():
     d2h = int(pin_pix.numel() * 4 + pin_dep.numel() * 4)
 
     # max over ranks
-    times = torch.tensor([total_ms, e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_s = float(times[0]), float(times[1])
-    value = rays_per_frame * args.steps * world / (total_ms / 1000.0) / 1e6
-    e2e_value = rays_per_frame * args.steps * world / e2e_s / 1e6
+    total_ms, e2e_s = max_over_ranks([total_ms, e2e_s], dev, world)
+    value = whole_job_rate(rays_per_frame, args.steps, world, total_ms)
+    e2e_value = whole_job_rate(rays_per_frame, args.steps, world, e2e_s * 1000.0)
 
     # roofline of the dominant kernel
     timed = {k: v for k, v in stats.items() if v["launches"]}

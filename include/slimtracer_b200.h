@@ -340,7 +340,8 @@ int slimRefitSceneBVH(void *stream);
  * encoded as 12-octave sin/cos of p, bands 0..3 spherical harmonics of the
  * direction, normal, roughness, albedo and a constant 1.  Parameters: one
  * f32 vector of SLIM_NRC_PARAMS, W0 [64][96], W1..W3 [64][64], W4 [3][64]
- * (row = output unit).  Training: relative L2 loss, Adam. */
+ * (row = output unit).  Training: L2 on log(radiance + 0.01) against the
+ * exp output's argument, Adam; the cache answers max(exp(z) - 0.01, 0). */
 #define SLIM_NRC_PARAMS 18624
 #define SLIM_NRC_FEATURES 16
 typedef struct {
@@ -361,7 +362,7 @@ typedef struct {
     uint64_t frames, steps;  /* frames rendered with the cache, Adam steps taken */
     uint32_t queries;        /* cache queries of the last frame */
     uint32_t train_samples;  /* training samples of the last frame */
-    float loss;              /* mean relative-L2 loss of the last step */
+    float loss;              /* mean log-radiance L2 loss of the last step */
     float _pad;
 } SlimRadianceCacheStats;
 

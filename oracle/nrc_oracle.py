@@ -14,12 +14,12 @@ mixed precision step by step:
              [92,95)  albedo              [95] constant 1 (the first layer's bias)
   forward  four hidden layers of 64 ReLU units, no biases past the first:
              H_{l+1} = bf16(relu(H_l W_l^T))  with f32 accumulation,
-           output z = H_4 W_4^T (3 channels), radiance = exp(min(z, 15))
-  loss     relative L2 (Mueller et al. 2021, "Real-time Neural Radiance Caching
-           for Path Tracing"): (y' - y)^2 / (y'^2 + 0.01), y' held constant in
-           the denominator, averaged over samples and channels
-  backward per-sample output gradient dz = 2 (y' - y) y' / (y'^2 + 0.01) (0 where
-           z was clamped), rounded to bf16; hidden gradients
+           output z = H_4 W_4^T (3 channels), radiance = max(exp(min(z, 15)) - 0.01, 0)
+  loss     L2 in log space: (z - log(y + 0.01))^2, averaged over samples and
+           channels (z regresses log radiance; the gradient through an exp
+           output never vanishes, unlike a relative L2 on exp(z))
+  backward per-sample output gradient dz = 2 (z - log(y + 0.01)), rounded to
+           bf16; hidden gradients
            g_l = bf16(dH_l * [H_l > 0]),  dH_l = g_{l+1} W_l  (f32 accumulation);
            weight gradients dW_l = sum over samples of g^T H, divided by 3 * batch
   adam     Kingma & Ba 2015 with bias correction; the f32 master weights are
@@ -36,7 +36,7 @@ N_IN, N_HIDDEN, N_OUT = 96, 64, 3
 SHAPES = [(64, 96), (64, 64), (64, 64), (64, 64), (3, 64)]
 N_PARAMS = sum(a * b for a, b in SHAPES)
 OCTAVES = 12
-REL_EPS = 0.01
+LOG_OFFSET = 0.01
 Z_MAX = 15.0
 
 
@@ -115,7 +115,7 @@ def forward(params, X, rounding=True):
     for l in range(4):
         H.append(_round(np.maximum(H[-1] @ W[l].T, 0.0), rounding))
     z = H[-1] @ W[4].T
-    y = np.exp(np.minimum(z, Z_MAX))
+    y = np.maximum(np.exp(np.minimum(z, Z_MAX)) - LOG_OFFSET, 0.0)
     return {"H": H, "z": z, "y": y, "W": W}
 
 
@@ -124,12 +124,10 @@ def infer(params, features):
 
 
 def loss_and_output_gradient(fw, target):
-    y, z = fw["y"], fw["z"]
-    t = np.asarray(target, np.float64)[:, :3]
-    den = y * y + REL_EPS
-    loss = float(np.mean((y - t) ** 2 / den))
-    dz = np.where(z > Z_MAX, 0.0, 2.0 * (y - t) * y / den)
-    return loss, dz
+    z = fw["z"]
+    t = np.log(np.maximum(np.asarray(target, np.float64)[:, :3], 0.0) + LOG_OFFSET)
+    diff = z - t
+    return float(np.mean(diff * diff)), 2.0 * diff
 
 
 def gradients(params, features, target, rounding=True, X=None):

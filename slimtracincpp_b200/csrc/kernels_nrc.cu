@@ -9,7 +9,7 @@
 //
 //   infer  forward only; 80 KB of shared memory, 128 TMEM columns, persistent
 //          over tiles (grid = 2 CTAs per SM).
-//   train  forward, relative-L2 output gradient, backward; 162 KB of shared
+//   train  forward, log-radiance L2 output gradient, backward; 162 KB of shared
 //          memory (weights, the input tile, the four hidden tiles, two
 //          gradient tiles), 512 TMEM columns: the forward and input-gradient
 //          accumulators plus one accumulator per weight matrix that sums
@@ -251,8 +251,9 @@ __global__ void __launch_bounds__(128) k_nrc_infer(const float4 *__restrict__ fe
                 float z[16];
                 tmem_ld16w(lane + kColOut, z);
                 if (valid)
-                    radiance[i] = make_float4(expf(fminf(z[0], kZMax)), expf(fminf(z[1], kZMax)),
-                                              expf(fminf(z[2], kZMax)), 0.0f);
+                    radiance[i] = make_float4(fmaxf(expf(fminf(z[0], kZMax)) - kLogOffset, 0.0f),
+                                              fmaxf(expf(fminf(z[1], kZMax)) - kLogOffset, 0.0f),
+                                              fmaxf(expf(fminf(z[2], kZMax)) - kLogOffset, 0.0f), 0.0f);
             }
             sync_for_mma();
             if (abort_s) { aborted = true; break; }
@@ -356,11 +357,10 @@ __global__ void __launch_bounds__(128, 1) k_nrc_train(const float4 *__restrict__
                     const float tv[3] = {y.x, y.y, y.z};
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
-                        float e = expf(fminf(z[c], kZMax));
-                        float den = e * e + kRelEps;
-                        float diff = e - tv[c];
-                        loss += diff * diff / den;
-                        dz[c] = z[c] > kZMax ? 0.0f : 2.0f * diff * e / den;
+                        // L2 on log radiance: z regresses log(target + offset)
+                        float diff = z[c] - logf(fmaxf(tv[c], 0.0f) + kLogOffset);
+                        loss += diff * diff;
+                        dz[c] = 2.0f * diff;
                     }
                 }
                 float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};

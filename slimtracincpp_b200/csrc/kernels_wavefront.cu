@@ -511,7 +511,8 @@ __global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, Que
 SLIM_D unsigned long long hit_key(float t, uint32_t k) {
     return ((unsigned long long)__float_as_uint(t) << 32) | k;
 }
-constexpr unsigned long long kNoHitKey = ~0ull;
+// No hit yet: distance +inf (the culling bound reads the high word as a float).
+constexpr unsigned long long kNoHitKey = (0x7F800000ull << 32) | 0xFFFFFFFFull;
 
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256) k_extend_scene(DevScene S0, DevFrame F0, QueueArgs A) {

@@ -1,5 +1,8 @@
 // Neural radiance cache: a 96-64-64-64-64-3 MLP (ReLU hidden units, exp
-// output) evaluated and trained on the sm_100a tensor cores.  No counterpart
+// output) evaluated and trained on the sm_100a tensor cores.  The network's
+// raw output z regresses log(radiance + 0.01) (an L2 loss in log space, whose
+// gradient 2 (z - log(y + 0.01)) never vanishes, unlike a relative L2 through
+// the exp); the cache answers max(exp(z) - 0.01, 0).  No counterpart
 // in the reference: the cache answers for the radiance leaving a surface point
 // reached by a bounce ray, in place of the rest of the path.
 //
@@ -28,8 +31,8 @@ constexpr int kImgW = kHidden * kHidden * 2;        // 8192
 constexpr int kImgW4 = kOutPad * kHidden * 2;       // 2048
 constexpr int kImgOff1 = kImgW0, kImgOff4 = kImgW0 + 3 * kImgW;
 constexpr int kImgBytes = kImgW0 + 3 * kImgW + kImgW4;          // 38912
-constexpr float kRelEps = 0.01f;   // relative-L2 denominator offset
-constexpr float kZMax = 15.0f;     // exp(min(z, 15))
+constexpr float kLogOffset = 0.01f;  // z regresses log(radiance + 0.01); answers exp(z) - 0.01
+constexpr float kZMax = 15.0f;       // exp(min(z, 15))
 constexpr uint32_t kErrTimeout = 4u;
 
 struct AdamArgs {
@@ -52,7 +55,7 @@ cudaError_t launch_infer(const float4 *features, const uint32_t *count, uint32_t
 
 // One optimisation step over the (features, targets) pairs [offset, offset +
 // samples), clipped to *count when `count` (a device counter) is given:
-// gradients of the mean relative-L2 loss into grad (f32, kParams), Adam update
+// gradients of the mean log-radiance L2 loss into grad (f32, kParams), Adam update
 // of params / m / v, refreshed bf16 image, loss into *loss.  A step with no
 // samples changes nothing.
 cudaError_t launch_train_step(const float4 *features, const float4 *targets, uint32_t samples, const uint32_t *count,

@@ -2,9 +2,10 @@
 CPU oracle (oracle/nrc_oracle.py), and the cache inside a wavefront frame.
 
 Bars:
-  * forward: log-radiance within 0.05 of the oracle on every sample and
-    within 5e-3 on 99 % (bf16 activations: an f32 accumulation that lands on
-    a bf16 rounding boundary may round the other way than the oracle's);
+  * forward: the output z = log(radiance + 0.01) within 0.05 of the oracle's
+    on every sample and within 5e-3 on 99 % (bf16 activations: an f32
+    accumulation that lands on a bf16 rounding boundary may round the other
+    way than the oracle's);
   * gradients: relative error of every layer's gradient below 2 %;
   * Adam: the update of the GPU gradient within f32 rounding of the oracle's;
   * EXACT cache mode (every query traced on by the tracer): the plain frame
@@ -80,7 +81,8 @@ def test_query_matches_oracle(cache, n):
     f = rand_features(rng, n)
     got = query(cache, f)
     ref = N.infer(params, f)
-    err = np.abs(np.log(got) - np.log(ref))
+    # compared in the network's output space: log(radiance + 0.01) = z
+    err = np.abs(np.log(got + N.LOG_OFFSET) - np.log(ref + N.LOG_OFFSET))
     assert err.max() < 0.05, err.max()
     assert np.quantile(err, 0.99) < 5e-3
 
@@ -132,15 +134,15 @@ def test_online_training_fits_a_smooth_radiance(cache):
 
     def val_loss():
         y = query(cache, fv)
-        return float(np.mean((y - tv[:, :3]) ** 2 / (y * y + N.REL_EPS)))
+        return float(np.mean((np.log(y + N.LOG_OFFSET) - np.log(tv[:, :3] + N.LOG_OFFSET)) ** 2))
 
     before = val_loss()
     for it in range(300):
         o = (it % 16) * 4096
         cache.train(df[o:].data_ptr(), dt[o:].data_ptr(), 4096)
     after = val_loss()
-    assert after < 0.1 * before, (before, after)
-    assert after < 2e-3
+    assert after < 0.05 * before, (before, after)
+    assert after < 5e-3
 
 
 def renderer_for(w):

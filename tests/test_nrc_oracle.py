@@ -33,20 +33,19 @@ def test_param_count_matches_the_abi():
 
 
 def test_backward_matches_finite_differences():
-    """Exact (unrounded) mode: the analytic gradient of the relative-L2
-    surrogate (denominator held at the current output) against central
-    differences, for parameters of every layer."""
+    """Exact (unrounded) mode: the analytic gradient of the log-radiance L2
+    loss against central differences, for parameters of every layer."""
     rng = np.random.default_rng(0)
     params = rand_params(rng).astype(np.float64)
     f = rand_features(rng, 48)
     X = N.encode(f).astype(np.float64)
     target = rng.uniform(0.0, 2.0, (48, 4))
     grad, _ = N.gradients(params, f, target, rounding=False, X=X)
-    den0 = N.forward(params, X, rounding=False)["y"] ** 2 + N.REL_EPS
+    logt = np.log(target[:, :3] + N.LOG_OFFSET)
 
     def surrogate(p):
-        y = N.forward(p, X, rounding=False)["y"]
-        return np.mean((y - target[:, :3]) ** 2 / den0)
+        z = N.forward(p, X, rounding=False)["z"]
+        return np.mean((z - logt) ** 2)
 
     bounds = np.cumsum([0] + [a * b for a, b in N.SHAPES])
     idx = np.concatenate([rng.choice(np.arange(bounds[i], bounds[i + 1]), 8, replace=False) for i in range(5)])

@@ -310,6 +310,20 @@ int slimTracePrimary(const SlimCameraRayProjection *projection, int width, int h
                      void *d_geometry_ids, void *d_primitive_ids, void *d_distances,
                      void *d_from_behind, void *stream);
 
+/* Selection::manipulate's pick (scene/selection.h:36-80): the geometry
+ * behind pixel (x, y) and the point light whose selection sphere the ray
+ * reaches first (light >= 0 wins over the geometry, as in the reference).
+ * Synchronous. */
+typedef struct {
+    int32_t geometry;          /* closest geometry index, -1 on a miss */
+    int32_t light;             /* picked light index, -1 for none */
+    uint32_t triangle;         /* mesh triangle id in leaf order (0 for implicit primitives) */
+    float distance;            /* hit distance along the normalised ray (INF on a miss) */
+    float position[3];         /* world position of the hit */
+    uint32_t from_behind;
+} SlimPick;
+int slimPick(const SlimCameraRayProjection *projection, int x, int y, SlimPick *out);
+
 /* Work counters of the last frame rendered with options.count_work set. */
 int slimGetWorkCounters(SlimWorkCounters *counters);
 
@@ -433,6 +447,7 @@ SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheConfig) == 48, "RadianceCacheConfig i
 SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheStats) == 32, "RadianceCacheStats is 32 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRenderRequest) == 184, "RenderRequest is 184 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimBatchPlan) == 32, "BatchPlan is 32 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimPick) == 32, "Pick is 32 bytes");
 
 /* Host-side helpers: the reference's own host algorithms, restated. */
 

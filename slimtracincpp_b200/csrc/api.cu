@@ -170,7 +170,7 @@ struct EventTimer : StageTimer {
     }
 };
 const char *kStageNames[STAGE_COUNT] = {"fused", "extend", "shadow_gen", "shadow", "shade", "refit", "shadow_mesh",
-                                        "cache", "cache_train", "cache_query"};
+                                        "cache", "cache_train", "cache_query", "tail"};
 SlimWorkCounters g_stage_work[STAGE_COUNT];
 
 Context g_ctx;
@@ -878,6 +878,20 @@ int slimSynchronize(void *stream) {
     int rc = read_errors(c, (cudaStream_t)stream);
     if (rc) return rc;
     return read_counters(c, (cudaStream_t)stream);
+}
+
+int slimPick(const SlimCameraRayProjection *projection, int x, int y, SlimPick *out) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!projection || !out) return set_error(SLIM_ERR_ARGUMENT, "slimPick: null argument");
+    SlimPick *d = nullptr;
+    SLIM_CUDA(cudaMalloc(&d, sizeof(SlimPick)), "pick buffer");
+    cudaError_t e = launch_pick(c.scene, *projection, x, y, d, c.d_error.ptr, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(SlimPick), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "pick");
+    return read_errors(c, nullptr);
 }
 
 int slimSetRenderOptions(const SlimRenderOptions *options) {

@@ -10,7 +10,7 @@ namespace slim {
 // slots per stage in DevFrame::counters).
 enum Stage : int {
     STAGE_FUSED = 0, STAGE_EXTEND, STAGE_SHADOW_GEN, STAGE_SHADOW, STAGE_SHADE, STAGE_REFIT, STAGE_SHADOW_MESH,
-    STAGE_CACHE, STAGE_CACHE_TRAIN, STAGE_CACHE_QUERY, STAGE_COUNT
+    STAGE_CACHE, STAGE_CACHE_TRAIN, STAGE_CACHE_QUERY, STAGE_TAIL, STAGE_COUNT
 };
 constexpr int kCountersPerStage = 16;
 
@@ -29,6 +29,10 @@ cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block,
 cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjection &P, uint32_t width, uint32_t height,
                                  int *geometry_ids, uint32_t *primitive_ids, float *distances, uint8_t *from_behind,
                                  uint32_t *error_flags, cudaStream_t stream);
+
+// Single-ray pick behind a pixel (scene/selection.h:36-80) into device `out`.
+cudaError_t launch_pick(const DevScene &S, const SlimCameraRayProjection &P, int x, int y, SlimPick *out,
+                        uint32_t *error_flags, cudaStream_t stream);
 
 // Wavefront form: stage kernels over compacted ray queues.
 struct WavefrontBuffers {

@@ -162,7 +162,64 @@ __global__ void __launch_bounds__(128) k_trace_primary(DevScene S, SlimCameraRay
     if (err) atomicOr(error_flags, err);
 }
 
+// Selection::manipulate's pick (scene/selection.h:36-80): the closest
+// geometry behind pixel (x, y), then every point light's selection sphere
+// (radius intensity / 2 / 64) along the same -- already offset -- ray up to
+// the hit distance, each hit shrinking that distance; the last light hit
+// wins over the geometry.  One thread.
+__global__ void k_pick(DevScene S, SlimCameraRayProjection P, int x, int y, SlimPick *out, uint32_t *error_flags) {
+    if (blockIdx.x || threadIdx.x) return;
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    Ray ray;
+    reset(ray, f3(P.camera_position.x, P.camera_position.y, P.camera_position.z), normalized(primary_direction(P, x, y)));
+    Hit hit;
+    int g = scene_trace<false>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+    float max_distance = hit.distance;
+    int light = -1;
+    for (uint32_t i = 0; i < S.light_count; i++) {
+        LightRec l = load_light(S, i);
+        if (l.flags & SLIM_LIGHT_IS_DIRECTIONAL) continue;
+        // SphereTracer::hit (core/ray.h:317-336)
+        float radius = l.intensity * 0.5f * kLightIntensityRadius;
+        float orr = kLightRadiusIntensity / (l.intensity * 0.5f);
+        float t_max = max_distance * orr;
+        float3 rc = (l.pos - ray.o) * orr;
+        float b = dot(ray.d, rc);
+        float c = sqlen(rc) - 1;
+        float h = b * b - c;
+        if (h >= 0) {
+            h = sqrtf(h);
+            float t_near = b - h, t_far = b + h;
+            if (t_far > 0 && t_near < t_max) {
+                max_distance = t_max * radius;
+                light = (int)i;
+            }
+        }
+    }
+    SlimPick r;
+    r.geometry = g;
+    r.light = light;
+    r.triangle = (g >= 0 && load_geo(S, (uint32_t)g).type == SLIM_GEOMETRY_MESH) ? hit.id : 0u;
+    r.distance = g >= 0 ? hit.distance : INFINITY;
+    float3 pos = g >= 0 ? at(ray, hit.distance) : f3(0, 0, 0);
+    r.position[0] = pos.x;
+    r.position[1] = pos.y;
+    r.position[2] = pos.z;
+    r.from_behind = g >= 0 ? (uint32_t)hit.from_behind : 0u;
+    *out = r;
+    if (err) atomicOr(error_flags, err);
+}
+
 }  // namespace dev
+
+cudaError_t launch_pick(const DevScene &S, const SlimCameraRayProjection &P, int x, int y, SlimPick *out,
+                        uint32_t *error_flags, cudaStream_t stream) {
+    dev::k_pick<<<1, 32, 0, stream>>>(S, P, x, y, out, error_flags);
+    count_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
                                 StageTimer *timer) {

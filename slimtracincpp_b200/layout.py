@@ -99,6 +99,8 @@ CACHE_OFF, CACHE_ON, CACHE_TRUNCATE, CACHE_EXACT = 0, 1, 2, 3
 RENDER_REQUEST = _dt([("scene", u8, 0), ("projection", PROJECTION, 8), ("settings", SETTINGS, 108),
                       ("width", u4, 152), ("height", u4, 156), ("radiance_cache", i4, 160), ("_pad", u4, 164),
                       ("d_pixels", u8, 168), ("d_depths", u8, 176)], 184)
+PICK = _dt([("geometry", i4, 0), ("light", i4, 4), ("triangle", u4, 8), ("distance", f4, 12),
+            ("position", (f4, 3), 16), ("from_behind", u4, 28)], 32)
 BATCH_PLAN = _dt([("queue_capacity", u4, 0), ("tile_pixels", u4, 4), ("block_size", i4, 8), ("waves", u4, 12),
                   ("batch_ms", f4, 16), ("candidates", u4, 20), ("graph_nodes", u4, 24), ("tuned", u4, 28)], 32)
 NRC_PARAMS = 18624

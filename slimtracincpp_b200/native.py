@@ -29,7 +29,7 @@ EXPORTS = [
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
     "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimSynchronize",
-    "slimGetLaunchCount",
+    "slimGetLaunchCount", "slimPick",
     "slimBatchSetRequests", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender",
 ]
 
@@ -84,6 +84,7 @@ def lib():
     for name in ["slimSynchronize", "slimRadianceCacheJoin", "slimGetLaunchCount", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender"]:
         getattr(h, name).argtypes = [P]
     h.slimBatchSetRequests.argtypes = [P, C.c_uint32]
+    h.slimPick.argtypes = [P, C.c_int, C.c_int, P]
     h.slimRadianceCacheTrain.argtypes = [P, P, C.c_uint32, P]
     for name in EXPORTS:
         if name not in ("slimGetLastError",):
@@ -155,3 +156,10 @@ def launch_count():
     n = np.zeros(1, np.uint64)
     check(lib().slimGetLaunchCount(ptr(n)))
     return int(n[0])
+
+
+def pick(projection, x, y):
+    """Selection::manipulate's pick behind pixel (x, y) (scene/selection.h:36-80)."""
+    out = np.zeros((), L.PICK)
+    check(lib().slimPick(ptr(projection), int(x), int(y), ptr(out)))
+    return out

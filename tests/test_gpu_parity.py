@@ -183,3 +183,44 @@ def test_normal_map_debug_mode(engine):
     st = L.default_settings(max_depth=3, render_mode=L.RENDER_NORMAL_MAP)
     opix, _, _ = O.oracle_render(w.scene, w.projection(), st, w.width, w.height, layout=L)
     assert np.array_equal(pix.view(np.uint32), opix.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["config1", "mesh_small", "features"])
+def test_pick_matches_the_closest_hit(name):
+    """slimPick's geometry, triangle, distance and side equal the oracle's
+    closest hit of the same pixel (bit for bit)."""
+    w = workloads()[name]()
+    RayTracingRenderer(w.scene, max_depth=int(w.settings["max_depth"]))
+    proj = w.projection()
+    og, op, od, ob = O.oracle_trace_primary(w.scene, proj, w.width, w.height)
+    rng = np.random.default_rng(0)
+    for _ in range(40):
+        x, y = int(rng.integers(0, w.width)), int(rng.integers(0, w.height))
+        i = y * w.width + x
+        p = native.pick(proj, x, y)
+        assert int(p["geometry"]) == og[i]
+        if og[i] >= 0:
+            assert int(p["triangle"]) == op[i]
+            assert np.float32(p["distance"]).view(np.uint32) == od[i].view(np.uint32)
+            assert int(p["from_behind"]) == ob[i]
+
+
+def test_pick_selects_a_light_in_front_of_the_geometry():
+    w = scenes.config1(2, 160, 90)
+    w.scene.lights[0]["position"] = (0.0, 3.0, -6.0)    # in front of the camera, above the floor
+    w.scene.lights[0]["intensity"] = 50.0                 # selection radius 50 / 2 / 64: a few pixels wide
+    RayTracingRenderer(w.scene, max_depth=1)
+    proj = w.projection()
+    light = w.scene.lights[0]
+    # the pixel whose ray points closest to the light's centre
+    P = proj
+    xs, ys = np.meshgrid(np.arange(w.width, dtype=np.float32), np.arange(w.height, dtype=np.float32))
+    d = (P["start"][None, None, :] + P["down"][None, None, :] * ys[..., None] + P["right"][None, None, :] * xs[..., None])
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    to_light = np.asarray(light["position"], np.float64) - np.asarray(P["camera_position"], np.float64)
+    to_light /= np.linalg.norm(to_light)
+    y, x = np.unravel_index(np.argmax(d @ to_light), d.shape[:2])
+    p = native.pick(proj, int(x), int(y))
+    assert int(p["light"]) == 0
+    far = native.pick(proj, 0, w.height - 1)
+    assert int(far["light"]) == -1

@@ -185,13 +185,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms), "source": "nvidia-smi -lms 200"}
 
 
-def algorithmic_bytes(w):
-    """Bytes the path must touch per frame (memory-hierarchy roofline):
-    32 B per BVH node test, 64 B per triangle test, 64 B per mesh-hit
-    attribute fetch, 72 B per instance test, 16 B per texel-quad tap, plus
-    20 B per sample of framebuffer written."""
+def algorithmic_bytes(w, pixels=None):
+    """Bytes the path must touch (memory-hierarchy roofline): 32 B per BVH
+    node test, 64 B per triangle test, 64 B per mesh-hit attribute fetch,
+    72 B per instance test, 16 B per texel-quad tap, plus 20 B per pixel of
+    framebuffer written (a frame: one per primary ray; a stage: `pixels`)."""
+    fb = w["primary_rays"] if pixels is None else pixels
     return (32 * (w["scene_node_tests"] + w["mesh_node_tests"]) + 64 * w["triangle_tests"] +
-            64 * w["mesh_hit_fetches"] + 72 * w["geometry_tests"] + 16 * w["texel_taps"] + 20 * w["primary_rays"])
+            64 * w["mesh_hit_fetches"] + 72 * w["geometry_tests"] + 16 * w["texel_taps"] + 20 * fb)
+
+
+# DRAM bytes (read + write) per launch of a stage, measured with
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
+# on the bench's own command (profiles/ holds the per-kernel table).  ncu flushes caches before every kernel, so
+# these are cold-cache bytes.  A stage launch is all kernels of one round: extend = scene + mesh + resolve + overflow.
+TRAFFIC_BYTES_PER_LAUNCH = {
+    ("config2", "extend"): 180.0e6,       # rounds 1 and 2: 259 MB and 101 MB
+    ("config2", "shadow_mesh"): 61.7e6,   # 92.9 MB and 29.9 MB
+}
+PIXEL_STAGES = ("shade", "tail", "fused")   # stages that write the framebuffer
 
 
 def measured_peaks():
@@ -693,11 +705,14 @@ def main():
         d = timed[dom_name]
         per_launch_ms = d["total_ms"] / d["launches"]
         launches_per_frame = d["launches"] / args.steps
-        alg = algorithmic_bytes(stage_work[dom_name]) / max(1.0, launches_per_frame)
+        px = work["primary_rays"] if dom_name in PIXEL_STAGES else 0
+        alg = algorithmic_bytes(stage_work[dom_name], px) / max(1.0, launches_per_frame)
         achieved = alg / (per_launch_ms / 1000.0) / 1e9
         roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                    "traffic": None, "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
+                    "traffic": TRAFFIC_BYTES_PER_LAUNCH.get((args.config, dom_name)),
+                    "traffic_note": "ncu dram read+write per stage launch, cold caches",
+                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
                     "share_of_frame": d["total_ms"] / total_ms}
     frame_bytes = algorithmic_bytes(work)
 

@@ -457,6 +457,18 @@ struct PendingLeaves {
     SLIM_D bool can_step() const { return n <= kStepWhileWaiting; }
 };
 
+// Warp-uniform decision: should idle lanes take new candidates now?  Idle
+// lanes wait until a quarter of the warp is idle (or nobody is busy) and
+// then fetch together, so the fetch code -- one atomic, the candidate loads,
+// the ray set-up -- runs for several lanes at once instead of for the one or
+// two that finished this turn (config 2: 1.94 -> 1.82 ms).
+constexpr uint32_t kFetchFraction = 4;   // fetch when idle lanes >= active lanes / kFetchFraction
+SLIM_D bool fetch_round(bool idle) {
+    const uint32_t act = __activemask();
+    const uint32_t idle_mask = __ballot_sync(act, idle);
+    return idle_mask && (kFetchFraction * (uint32_t)__popc(idle_mask) >= (uint32_t)__popc(act) || idle_mask == act);
+}
+
 // Warp-uniform decision: test waiting leaves now?
 SLIM_D bool leaf_round(bool waiting, bool can_step) {
     const uint32_t act = __activemask();
@@ -479,7 +491,8 @@ __global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, Que
     PendingLeaves pend;
     pend.n = 0;
     for (;;) {
-        if (!busy) {
+        const bool fetch = fetch_round(!busy);
+        if (!busy && fetch) {
             uint32_t active = __activemask();
             int leader = __ffs(active) - 1;
             uint32_t base = 0;
@@ -754,7 +767,8 @@ __global__ void __launch_bounds__(256) k_extend_mesh(DevScene S, DevFrame F, Que
     PendingLeaves pend;
     pend.n = 0;
     for (;;) {
-        if (!busy) {
+        const bool fetch = fetch_round(!busy);
+        if (!busy && fetch) {
             uint32_t active = __activemask();
             int leader = __ffs(active) - 1;
             uint32_t base = 0;

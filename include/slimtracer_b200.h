@@ -200,6 +200,13 @@ typedef struct {
                                 nothing (the method without the network); EXACT: every
                                 query traced on to max_depth by the tracer (a check of the
                                 cache plumbing: equals the plain frame up to rounding) */
+    int32_t row_bands;       /* wavefront frames render in this many row bands, two in flight
+                                at once (the caller's stream and a second one), so one
+                                band's launch tails overlap the other's work; into a pinned
+                                host canvas each band downloads while the next renders.
+                                0 = default (2 from 512x512 samples up, else 1), 1 = whole
+                                frame, at most 64.  Radiance-cache frames and the fused
+                                engine use one band.  The pixels are the same either way. */
 } SlimRenderOptions;
 enum { SLIM_CACHE_OFF = 0, SLIM_CACHE_ON = 1, SLIM_CACHE_TRUNCATE = 2, SLIM_CACHE_EXACT = 3 };
 
@@ -229,6 +236,7 @@ SLIM_STATIC_ASSERT(sizeof(SlimSceneData) == 184, "SceneData is 184 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimCanvasData) == 56, "CanvasData is 56 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimCameraRayProjection) == 100, "CameraRayProjection is 100 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRayTracerSettings) == 44, "RayTracerSettings is 44 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimRenderOptions) == 36, "RenderOptions is 36 bytes");
 
 /* ======================================================================== *
  * Drop-in hooks (renderer/renderer_GPU.h)                                   *

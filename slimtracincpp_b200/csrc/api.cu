@@ -65,6 +65,9 @@ struct Context {
     bool initialized = false;
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;          // banded downloads
+    cudaEvent_t refit_done = nullptr;            // the last scene BVH refit, on the caller's stream
+    std::vector<cudaEvent_t> band_events;        // one per band, the last marks the downloads' end
     SlimSceneCounts counts{};
     std::vector<SlimGeometry> geometries;
     std::vector<SlimMaterial> materials;
@@ -88,11 +91,16 @@ struct Context {
     DevScene scene{};
     SlimRenderOptions options{};
     SlimWorkCounters last_counters{};
-    WavefrontBuffers wavefront{};
-    DevArray<float4> w_color, w_through, w_rays0, w_rays1, w_hits, w_shadow_rays;
-    DevArray<uint32_t> w_counts;
-    DevArray<unsigned long long> w_shadow_mask;
-    DevArray<float4> w_pairs;
+    // Queues of the wavefront engine: two sets, so two row bands of a frame
+    // can be in flight at once (one on the caller's stream, one on band_stream).
+    struct WaveSet {
+        DevArray<float4> color, through, rays0, rays1, hits, shadow_rays, pairs;
+        DevArray<uint32_t> counts;
+        DevArray<unsigned long long> mask;
+        WavefrontBuffers B{};
+    } wave[2];
+    cudaStream_t band_stream = nullptr;
+    cudaEvent_t band_fork = nullptr, band_join = nullptr;
     struct EventTimer *timer = nullptr;
 
     // neural radiance cache
@@ -515,7 +523,7 @@ int check_settings(const Context &c, const SlimRayTracerSettings *st) {
     return SLIM_OK;
 }
 
-int ensure_wavefront(Context &c, uint32_t samples);
+int ensure_wavefront(Context &c, uint32_t samples, int set);
 
 // Buffers and per-frame parameters of a radiance-cache frame.
 int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
@@ -603,13 +611,30 @@ StageTimer *timer_for(Context &c) {
     return c.timer;
 }
 
+// A frame reads the scene BVH that the last slimRefitSceneBVH wrote, on
+// whatever stream that ran.  A stream being captured into a graph is left
+// alone: a captured wait on an event recorded outside the capture is an
+// error, and the caller orders the graph's launch.
+int wait_for_refit(Context &c, cudaStream_t stream) {
+    if (!c.refit_done) return SLIM_OK;
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    SLIM_CUDA(cudaStreamIsCapturing(stream, &capture), "capture status");
+    if (capture == cudaStreamCaptureStatusNone) SLIM_CUDA(cudaStreamWaitEvent(stream, c.refit_done, 0), "wait for the refit");
+    return SLIM_OK;
+}
+
+// Renders the sample rows [row_begin, row_begin + rows) of the canvas (rows
+// 0: all of them); `first` clears the work counters (the first band of a
+// frame).
 int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
-           const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream) {
+           const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream,
+           uint32_t row_begin, uint32_t rows, bool first, int set = 0) {
     const SlimDimensions &dim = canvas->dimensions;
     if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
     if (canvas->antialias < SLIM_AA_NONE || canvas->antialias > SLIM_AA_SSAA) return set_error(SLIM_ERR_ARGUMENT, "bad antialias mode");
     int rc = check_settings(c, settings);
     if (rc) return rc;
+    if ((rc = wait_for_refit(c, stream))) return rc;
     uint32_t s = canvas->antialias == SLIM_AA_SSAA ? 2 : 1;
     DevFrame F;
     memset(&F, 0, sizeof(F));
@@ -617,6 +642,10 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     F.settings = *settings;
     F.width = (uint32_t)dim.width * s;
     F.height = (uint32_t)dim.height * s;
+    if (rows == 0) { row_begin = 0; rows = F.height; }
+    if (row_begin >= F.height || rows > F.height - row_begin) return set_error(SLIM_ERR_ARGUMENT, "band outside the canvas");
+    F.row_begin = row_begin;
+    F.rows = rows;
     F.stride = dim.stride ? dim.stride : dim.width;
     if (F.stride < dim.width) return set_error(SLIM_ERR_ARGUMENT, "canvas stride below width");
     F.antialias = canvas->antialias;
@@ -625,7 +654,7 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     F.depths = d_depths;
     F.error_flags = c.d_error.ptr;
     F.counters = c.options.count_work ? c.d_counters.ptr : nullptr;
-    if (F.counters)
+    if (F.counters && first)
         SLIM_CUDA(cudaMemsetAsync(F.counters, 0, kCountersPerStage * STAGE_COUNT * sizeof(unsigned long long), stream),
                   "clear counters");
     StageTimer *timer = timer_for(c);
@@ -633,21 +662,22 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) {
         e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer);
     } else {
-        rc = ensure_wavefront(c, F.width * F.height);
+        rc = ensure_wavefront(c, F.width * F.rows, set);
         if (rc) return rc;
         CacheFrame cf;
         const CacheFrame *cache = nullptr;
         if (c.options.radiance_cache != SLIM_CACHE_OFF) {
-            if ((rc = cache_frame(c, F.width * F.height, cf))) return rc;
+            if ((rc = cache_frame(c, F.width * F.rows, cf))) return rc;
             cache = &cf;
         }
-        e = launch_render_wavefront(c.scene, F, c.wavefront, c.options.block_size, stream, timer, cache);
+        e = launch_render_wavefront(c.scene, F, c.wave[set].B, c.options.block_size, stream, timer, cache);
     }
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return SLIM_OK;
 }
 
-int ensure_wavefront(Context &c, uint32_t samples) {
+int ensure_wavefront(Context &c, uint32_t samples, int set) {
+    Context::WaveSet &W = c.wave[set];
     size_t lights = c.scene.light_count ? c.scene.light_count : 1;
     size_t budget = (size_t)(c.options.shadow_queue_mb > 0 ? c.options.shadow_queue_mb : 1024) << 20;
     size_t shadow = (size_t)samples * lights;
@@ -655,39 +685,37 @@ int ensure_wavefront(Context &c, uint32_t samples) {
     if (shadow > max_shadow) shadow = max_shadow < samples ? samples : max_shadow;
     if (shadow > 0xFFFFFFFFull) shadow = 0xFFFFFFFFull;
     if ((uint64_t)samples << 6 > 0xFFFFFFFFull) return set_error(SLIM_ERR_LIMIT, "frame too large for the wavefront queues");
-    size_t meshes = c.scene.mesh_count ? c.scene.mesh_count : 1;
     size_t instances = 0;
     for (const SlimGeometry &g : c.geometries) instances += g.type == SLIM_GEOMETRY_MESH;
     size_t pairs = shadow * (instances < 4 ? (instances ? instances : 1) : 4);
     size_t max_pairs = budget / (3 * sizeof(float4));
     if (pairs > max_pairs) pairs = max_pairs;
     if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
-    (void)meshes;
-    if (c.wavefront.capacity >= samples && c.wavefront.shadow_capacity >= shadow && c.wavefront.pair_capacity >= pairs)
+    if (W.B.capacity >= samples && W.B.shadow_capacity >= shadow && W.B.pair_capacity >= pairs)
         return SLIM_OK;
     uint32_t n = samples;
     int rc = 0;
-    if ((rc = c.w_color.reserve(n, "alloc path colour"))) return rc;
-    if ((rc = c.w_through.reserve(n, "alloc path throughput"))) return rc;
-    if ((rc = c.w_rays0.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
-    if ((rc = c.w_rays1.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
-    if ((rc = c.w_hits.reserve(3 * (size_t)n, "alloc hit records"))) return rc;
-    if ((rc = c.w_shadow_rays.reserve(2 * shadow, "alloc shadow queue"))) return rc;
-    if ((rc = c.w_counts.reserve(8, "alloc queue counters"))) return rc;
-    if ((rc = c.w_shadow_mask.reserve(n, "alloc shadow masks"))) return rc;
-    if ((rc = c.w_pairs.reserve(3 * (pairs ? pairs : 1), "alloc shadow candidate pairs"))) return rc;
-    WavefrontBuffers &B = c.wavefront;
-    B.path_color = c.w_color.ptr;
-    B.path_throughput = c.w_through.ptr;
-    B.rays[0] = c.w_rays0.ptr;
-    B.rays[1] = c.w_rays1.ptr;
-    B.queue_count = c.w_counts.ptr;
-    B.hits = c.w_hits.ptr;
-    B.shadow_rays = c.w_shadow_rays.ptr;
-    B.shadow_mask = c.w_shadow_mask.ptr;
+    if ((rc = W.color.reserve(n, "alloc path colour"))) return rc;
+    if ((rc = W.through.reserve(n, "alloc path throughput"))) return rc;
+    if ((rc = W.rays0.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
+    if ((rc = W.rays1.reserve(2 * (size_t)n, "alloc ray queue"))) return rc;
+    if ((rc = W.hits.reserve(3 * (size_t)n, "alloc hit records"))) return rc;
+    if ((rc = W.shadow_rays.reserve(2 * shadow, "alloc shadow queue"))) return rc;
+    if ((rc = W.counts.reserve(8, "alloc queue counters"))) return rc;
+    if ((rc = W.mask.reserve(n, "alloc shadow masks"))) return rc;
+    if ((rc = W.pairs.reserve(3 * (pairs ? pairs : 1), "alloc shadow candidate pairs"))) return rc;
+    WavefrontBuffers &B = W.B;
+    B.path_color = W.color.ptr;
+    B.path_throughput = W.through.ptr;
+    B.rays[0] = W.rays0.ptr;
+    B.rays[1] = W.rays1.ptr;
+    B.queue_count = W.counts.ptr;
+    B.hits = W.hits.ptr;
+    B.shadow_rays = W.shadow_rays.ptr;
+    B.shadow_mask = W.mask.ptr;
     B.capacity = n;
     B.shadow_capacity = (uint32_t)shadow;
-    B.pairs = c.w_pairs.ptr;
+    B.pairs = W.pairs.ptr;
     B.pair_capacity = (uint32_t)pairs;
     return SLIM_OK;
 }
@@ -724,6 +752,115 @@ int read_counters(Context &c, cudaStream_t stream) {
         w.geometry_tests += p[6]; w.mesh_hit_fetches += p[7]; w.texel_taps += p[8];
     }
     w.pixels = w.primary_rays;
+    return SLIM_OK;
+}
+
+// Row bands of a wavefront frame.  Each band is a complete wavefront pass
+// over its rows; bands alternate between the two queue sets, one on the
+// caller's stream and one on band_stream, so two bands are in flight at
+// once and the ends of one band's persistent launches, where most of the GPU
+// waits on a few long walks, overlap the other band's work.  Into a pinned
+// host canvas every band downloads as soon as it is done, while the next
+// renders.  The pixels are the same for any band count.
+constexpr uint32_t kDefaultRowBands = 2;
+constexpr uint32_t kMinBandedSamples = 1u << 18;
+
+uint32_t row_bands(const Context &c, uint32_t sample_rows, uint32_t samples) {
+    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL || c.options.radiance_cache != SLIM_CACHE_OFF) return 1;
+    uint32_t bands = c.options.row_bands ? (uint32_t)c.options.row_bands
+                                         : (samples >= kMinBandedSamples ? kDefaultRowBands : 1u);
+    const uint32_t tiles = sample_rows / 4;
+    if (bands > tiles) bands = tiles ? tiles : 1;
+    return bands;
+}
+
+bool pinned_host(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// The frame into d_pixels / d_depths on `stream`; with host_pixels set, it
+// also downloads into the host canvas (ordered before the end of `stream`).
+int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
+                 const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream,
+                 SlimPixel *host_pixels, float *host_depths, size_t pixel_count, size_t depth_count) {
+    const SlimDimensions &dim = canvas->dimensions;
+    if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
+    uint32_t stride = dim.stride ? dim.stride : dim.width;
+    const bool ssaa = canvas->antialias == SLIM_AA_SSAA;
+    const uint32_t sample_rows = (uint32_t)dim.height * (ssaa ? 2 : 1);
+    const uint32_t bands = row_bands(c, sample_rows, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1));
+    const bool download = host_pixels != nullptr;
+    int rc;
+    if (bands <= 1) {
+        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, stream, 0, 0, true))) return rc;
+        if (download) {
+            SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost,
+                                      stream), "download pixels");
+            SLIM_CUDA(cudaMemcpyAsync(host_depths, d_depths, depth_count * sizeof(float), cudaMemcpyDeviceToHost,
+                                      stream), "download depths");
+        }
+        return SLIM_OK;
+    }
+    // Canvas entries per sample row: a row of pixels (4 SSAA samples per
+    // pixel, two sample rows per canvas row) and of depths (4 per pixel
+    // under MSAA and SSAA).
+    const size_t pix_per_row = ssaa ? (size_t)stride * 2 : stride;
+    const size_t dep_per_row = ssaa ? (size_t)stride * 2 : (size_t)stride * (canvas->antialias == SLIM_AA_NONE ? 1 : 4);
+    const bool banded_download = download && pinned_host(host_pixels) && pinned_host(host_depths);
+    if (!c.band_stream) SLIM_CUDA(cudaStreamCreateWithFlags(&c.band_stream, cudaStreamNonBlocking), "band stream");
+    if (!c.band_fork) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_fork, cudaEventDisableTiming), "band event");
+    if (!c.band_join) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_join, cudaEventDisableTiming), "band event");
+    if (banded_download && !c.copy_stream)
+        SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking), "copy stream");
+    while (c.band_events.size() < bands + 1) {
+        cudaEvent_t e;
+        SLIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
+        c.band_events.push_back(e);
+    }
+    // Work counters are cleared once, before the fork; the band stream
+    // starts after everything the caller queued so far (the refit included).
+    if (c.options.count_work)
+        SLIM_CUDA(cudaMemsetAsync(c.d_counters.ptr, 0, kCountersPerStage * STAGE_COUNT * sizeof(unsigned long long),
+                                  stream), "clear counters");
+    if ((rc = wait_for_refit(c, stream))) return rc;
+    SLIM_CUDA(cudaEventRecord(c.band_fork, stream), "band fork");
+    SLIM_CUDA(cudaStreamWaitEvent(c.band_stream, c.band_fork, 0), "band fork");
+    const cudaStream_t lanes[2] = {stream, c.band_stream};
+    const uint32_t tiles = sample_rows / 4;
+    uint32_t r0 = 0;
+    for (uint32_t b = 0; b < bands; b++) {
+        const uint32_t r1 = b + 1 == bands ? sample_rows : 4 * (uint32_t)((uint64_t)tiles * (b + 1) / bands);
+        const cudaStream_t ls = lanes[b & 1];
+        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, (int)(b & 1))))
+            return rc;
+        if (banded_download) {
+            SLIM_CUDA(cudaEventRecord(c.band_events[b], ls), "band event");
+            SLIM_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_events[b], 0), "band wait");
+            const size_t p0 = pix_per_row * r0, pn = pix_per_row * (r1 - r0);
+            const size_t d0 = dep_per_row * r0, dn = dep_per_row * (r1 - r0);
+            SLIM_CUDA(cudaMemcpyAsync(host_pixels + p0, d_pixels + p0, pn * sizeof(float4), cudaMemcpyDeviceToHost,
+                                      c.copy_stream), "download pixels");
+            SLIM_CUDA(cudaMemcpyAsync(host_depths + d0, d_depths + d0, dn * sizeof(float), cudaMemcpyDeviceToHost,
+                                      c.copy_stream), "download depths");
+        }
+        r0 = r1;
+    }
+    SLIM_CUDA(cudaEventRecord(c.band_join, c.band_stream), "band join");
+    SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join, 0), "band join");
+    if (banded_download) {
+        SLIM_CUDA(cudaEventRecord(c.band_events[bands], c.copy_stream), "downloads done");
+        SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[bands], 0), "downloads done");
+    } else if (download) {
+        SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, stream),
+                  "download pixels");
+        SLIM_CUDA(cudaMemcpyAsync(host_depths, d_depths, depth_count * sizeof(float), cudaMemcpyDeviceToHost, stream),
+                  "download depths");
+    }
     return SLIM_OK;
 }
 
@@ -824,11 +961,9 @@ int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection 
     int rc = c.d_pixels.reserve(pixel_count, "alloc frame");
     if (rc) return rc;
     if ((rc = c.d_depths.reserve(depth_count, "alloc depths"))) return rc;
-    if ((rc = render(c, canvas, projection, settings, c.d_pixels.ptr, c.d_depths.ptr, c.stream))) return rc;
-    SLIM_CUDA(cudaMemcpyAsync(canvas->pixels, c.d_pixels.ptr, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, c.stream),
-              "download pixels");
-    SLIM_CUDA(cudaMemcpyAsync(canvas->depths, c.d_depths.ptr, depth_count * sizeof(float), cudaMemcpyDeviceToHost, c.stream),
-              "download depths");
+    if ((rc = render_frame(c, canvas, projection, settings, c.d_pixels.ptr, c.d_depths.ptr, c.stream, canvas->pixels,
+                           canvas->depths, pixel_count, depth_count)))
+        return rc;
     if ((rc = read_errors(c, c.stream))) return rc;
     return read_counters(c, c.stream);
 }
@@ -840,7 +975,8 @@ int slimRenderToDevice(const SlimCanvasData *canvas, const SlimCameraRayProjecti
     if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
     if (!canvas || !projection || !settings || !d_pixels || !d_depths)
         return set_error(SLIM_ERR_ARGUMENT, "slimRenderToDevice: null argument");
-    int rc = render(c, canvas, projection, settings, (float4 *)d_pixels, (float *)d_depths, (cudaStream_t)stream);
+    int rc = render_frame(c, canvas, projection, settings, (float4 *)d_pixels, (float *)d_depths, (cudaStream_t)stream,
+                          nullptr, nullptr, 0, 0);
     if (rc) return rc;
     if (c.options.count_work) {
         if ((rc = read_errors(c, (cudaStream_t)stream))) return rc;
@@ -900,7 +1036,7 @@ int slimSetRenderOptions(const SlimRenderOptions *options) {
     if (options->engine < 0 || options->engine > 1 || options->ray_cones < 0 || options->ray_cones > 1 ||
         options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 256 ||
         (options->block_size % 32) || options->radiance_cache < SLIM_CACHE_OFF ||
-        options->radiance_cache > SLIM_CACHE_EXACT)
+        options->radiance_cache > SLIM_CACHE_EXACT || options->row_bands < 0 || options->row_bands > 64)
         return set_error(SLIM_ERR_ARGUMENT, "bad render options");
     g_ctx.options = *options;
     return SLIM_OK;
@@ -927,6 +1063,9 @@ int slimRefitSceneBVH(void *stream) {
     cudaError_t e = launch_refit_scene_bvh(c.scene, c.d_scene_nodes.ptr, c.d_refit_order.ptr,
                                            (uint32_t)c.refit_order.size(), (cudaStream_t)stream, timer_for(c));
     if (e != cudaSuccess) return cuda_fail(e, "refit launch");
+    // the next frame, on whatever stream, reads the refit nodes
+    if (!c.refit_done) SLIM_CUDA(cudaEventCreateWithFlags(&c.refit_done, cudaEventDisableTiming), "refit event");
+    SLIM_CUDA(cudaEventRecord(c.refit_done, (cudaStream_t)stream), "refit event");
     return SLIM_OK;
 }
 
@@ -1082,6 +1221,7 @@ extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const Sli
     F.settings = *settings;
     F.width = (uint32_t)dim.width * s;
     F.height = (uint32_t)dim.height * s;
+    F.rows = F.height;
     F.stride = dim.stride ? dim.stride : dim.width;
     if (F.stride < dim.width) return set_error(SLIM_ERR_ARGUMENT, "canvas stride below width");
     F.antialias = canvas->antialias;
@@ -1094,10 +1234,11 @@ extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const Sli
     if ((rc = noalloc_scratch(&scratch))) return rc;
     WavefrontBuffers B;
     memset(&B, 0, sizeof(B));
-    if ((rc = noalloc_layout(scratch, F.width * F.height, c.scene.light_count, B))) return rc;
+    if ((rc = noalloc_layout(scratch, F.width * F.rows, c.scene.light_count, B))) return rc;
     // The queue counters at the head of the scratch are zeroed by the
     // launcher (cudaMemsetAsync) before the first stage reads them; every
     // other region is written before it is read within the frame.
+    if ((rc = wait_for_refit(c, (cudaStream_t)stream))) return rc;
     cudaError_t e = launch_render_wavefront(c.scene, F, B, c.options.block_size, (cudaStream_t)stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc render launch");
     return SLIM_OK;
@@ -1616,6 +1757,7 @@ int slimBatchSetRequests(const SlimRenderRequest *requests, uint32_t count) {
         F.settings = q.settings;
         F.width = q.width;
         F.height = q.height;
+        F.rows = q.height;
         F.stride = q.width;
         F.antialias = SLIM_AA_NONE;
         F.cones_per_pixel = c.options.ray_cones == SLIM_CONES_PER_PIXEL;

@@ -69,6 +69,7 @@ struct DevFrame {
     SlimCameraRayProjection projection;
     SlimRayTracerSettings settings;
     uint32_t width, height;        // sample grid (doubled under SSAA)
+    uint32_t row_begin, rows;      // the sample rows [row_begin, row_begin + rows) this launch renders
     uint32_t stride;               // canvas stride in pixels
     int32_t antialias;
     int32_t cones_per_pixel;

@@ -126,8 +126,8 @@ template <bool COUNT>
 __global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Work w = {};
-    if (i < F.width * F.height) {
-        int x = (int)(i % F.width), y = (int)(i / F.width);
+    if (i < F.width * F.rows) {
+        int x = (int)(i % F.width), y = (int)(F.row_begin + i / F.width);
         uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
         uint32_t err = 0;
         float3 color;
@@ -223,7 +223,7 @@ cudaError_t launch_pick(const DevScene &S, const SlimCameraRayProjection &P, int
 
 cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
                                 StageTimer *timer) {
-    uint32_t n = F.width * F.height;
+    uint32_t n = F.width * F.rows;
     if (block <= 0) block = 128;
     if (block > 128) block = 128;
     dim3 grid((n + block - 1) / block);

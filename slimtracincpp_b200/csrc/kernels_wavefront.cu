@@ -127,7 +127,6 @@ struct QueueArgs {
 // two differ for the radiance cache's training paths, whose state lives in
 // their own slots, and for batched paths, whose slots are per wave.
 constexpr uint32_t kBatchPixelBits = 23;
-constexpr uint32_t kBatchMaxRequests = 1u << (32 - kBatchPixelBits);
 
 template <bool BATCH> SLIM_D uint32_t req_of(uint32_t pid) { return BATCH ? pid >> kBatchPixelBits : 0u; }
 template <bool BATCH> SLIM_D uint32_t pix_of(uint32_t pid) {
@@ -177,7 +176,7 @@ SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float
                      uint32_t &pid) {
     if (!A.rays_in) {
         path = slot;
-        pid = pixel_of_slot(F.width, F.height, slot);
+        pid = F.row_begin * F.width + pixel_of_slot(F.width, F.rows, slot);
         primary_ray(F, pid, o, d);
         return;
     }
@@ -364,8 +363,10 @@ SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t tag, uin
     return false;
 }
 
+// Capped at 64 registers (4 blocks per SM instead of 3): latency-bound, the
+// extra warps pay for the few spills (config 2: shadow 0.157 -> 0.149 ms).
 template <bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256) k_shadow_scene(DevScene S0, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(256, 4) k_shadow_scene(DevScene S0, DevFrame F, QueueArgs A) {
     uint32_t n = *A.shadow_count;
     uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
     uint32_t err = 0;
@@ -1048,8 +1049,10 @@ SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], floa
 }
 
 // ---- shade: colour of this segment, next bounce, finished paths --------
+// Capped at 80 registers (3 blocks per SM instead of 2): latency-bound, the
+// extra warps pay for the spills (config 2: shade 0.180 -> 0.173 ms).
 template <bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
+__global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
     Work w = {};
     uint32_t stride = gridDim.x * blockDim.x;
@@ -1507,7 +1510,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
 template <bool COUNT>
 cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block, cudaStream_t stream,
                       StageTimer *timer, const CacheFrame *cache) {
-    uint32_t samples = F.width * F.height;
+    uint32_t samples = F.width * F.rows;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -89,7 +89,7 @@ SETTINGS = _dt([("max_depth", u1, 0), ("skybox_color_texture_id", i1, 1), ("skyb
                 ("skybox_irradiance_texture_id", i1, 3), ("render_mode", i4, 4), ("mip_level_colors", (i4, 9), 8)], 44)
 RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4, 8), ("block_size", i4, 12),
                       ("count_work", i4, 16), ("profile_stages", i4, 20), ("shadow_queue_mb", i4, 24),
-                      ("radiance_cache", i4, 28)], 32)
+                      ("radiance_cache", i4, 28), ("row_bands", i4, 32)], 36)
 CACHE_CONFIG = _dt([("cache_depth", u4, 0), ("train_samples", u4, 4), ("batch", u4, 8), ("seed", u4, 12),
                     ("learning_rate", f4, 16), ("beta1", f4, 20), ("beta2", f4, 24), ("epsilon", f4, 28),
                     ("train", u4, 32), ("overlap", u4, 36), ("_reserved", (u4, 2), 40)], 48)

@@ -120,12 +120,12 @@ def projection_reset(orientation9, position3, focal_length, width, height, ssaa=
 
 def set_render_options(engine=L.ENGINE_WAVEFRONT, ray_cones=L.CONES_REFERENCE, scene_bvh=L.SCENE_BVH_UPLOADED,
                        block_size=0, count_work=False, profile_stages=False, shadow_queue_mb=0,
-                       radiance_cache=L.CACHE_OFF):
+                       radiance_cache=L.CACHE_OFF, row_bands=0):
     o = np.zeros((), L.RENDER_OPTIONS)
     o["engine"], o["ray_cones"], o["scene_bvh"] = engine, ray_cones, scene_bvh
     o["block_size"], o["count_work"] = block_size, int(bool(count_work))
     o["profile_stages"], o["shadow_queue_mb"] = int(bool(profile_stages)), shadow_queue_mb
-    o["radiance_cache"] = radiance_cache
+    o["radiance_cache"], o["row_bands"] = radiance_cache, row_bands
     check(lib().slimSetRenderOptions(ptr(o)))
 
 

@@ -224,3 +224,68 @@ def test_pick_selects_a_light_in_front_of_the_geometry():
     assert int(p["light"]) == 0
     far = native.pick(proj, 0, w.height - 1)
     assert int(far["light"]) == -1
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("antialias", [L.AA_NONE, L.AA_MSAA, L.AA_SSAA])
+def test_banded_download_into_a_pinned_canvas(engine, antialias):
+    """slimRenderOnGPU renders the frame in row bands, two in flight on two
+    streams, and into pinned host memory downloads each band while the next
+    renders: the canvas must equal the one-band frame bit for bit, for any
+    band count (70 rows: the last band also holds the rows past the last
+    4-row tile band)."""
+    from slimtracincpp_b200.renderer import make_canvas
+    w = scenes.small_mesh_scene(0, 120, 70)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height, antialias)
+    native.set_render_options(engine=engine)
+    ref_pix, ref_dep = r.render(vp)          # pageable canvas: one download after the frame
+    cv, pix, dep = make_canvas(w.width, w.height, antialias)
+    pin_pix = torch.from_numpy(pix).pin_memory()
+    pin_dep = torch.from_numpy(dep).pin_memory()
+    cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
+    proj = w.camera.projection(w.width, w.height, antialias == L.AA_SSAA)
+    try:
+        for bands in (0, 1, 3, 64):
+            native.set_render_options(engine=engine, row_bands=bands)
+            pin_pix.fill_(-1.0)
+            pin_dep.fill_(-1.0)
+            native.check(native.lib().slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
+            assert np.array_equal(pin_pix.numpy().view(np.uint32), ref_pix.view(np.uint32)), bands
+            assert np.array_equal(pin_dep.numpy().view(np.uint32), ref_dep.view(np.uint32)), bands
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+
+
+
+def test_row_bands_on_the_callers_stream_with_work_counters():
+    """slimRenderToDevice with the frame split into row bands on the caller's
+    stream and a second one: same pixels and depths as the whole frame, the
+    same rays and scene-node tests.  Mesh-node and triangle tests depend on
+    the order in which concurrent candidates of a ray publish their hits
+    (culling), so they match only closely."""
+    w = scenes.small_mesh_scene(1, 160, 96)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    n = w.width * w.height
+    stream = torch.cuda.Stream()
+    results = []
+    try:
+        for bands in (1, 2, 5):
+            native.set_render_options(engine=L.ENGINE_WAVEFRONT, row_bands=bands, count_work=True)
+            pix = torch.full((n, 4), -1.0, device="cuda")
+            dep = torch.full((n,), -1.0, device="cuda")
+            torch.cuda.synchronize()
+            r.render_to_device(vp, pix.data_ptr(), dep.data_ptr(), stream.cuda_stream)
+            stream.synchronize()
+            results.append((pix.cpu().numpy(), dep.cpu().numpy(), native.work_counters()))
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    for pix, dep, work in results[1:]:
+        assert np.array_equal(pix.view(np.uint32), results[0][0].view(np.uint32))
+        assert np.array_equal(dep.view(np.uint32), results[0][1].view(np.uint32))
+        ref = results[0][2]
+        for k in ("primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "pixels"):
+            assert work[k] == ref[k], k
+        for k in ("mesh_node_tests", "triangle_tests"):
+            assert abs(work[k] - ref[k]) <= 0.02 * ref[k], k

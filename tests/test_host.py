@@ -42,6 +42,15 @@ def test_cuda_calls_fail_loudly_without_gpu_or_init():
     assert lib.slimGetLastError()
 
 
+def test_render_options_are_validated():
+    """Options outside their ranges are refused without touching the device."""
+    for bad in ({"row_bands": -1}, {"row_bands": 65}, {"block_size": 48}, {"radiance_cache": 4}):
+        with pytest.raises(native.SlimError):
+            native.set_render_options(**bad)
+    native.set_render_options(row_bands=64)
+    native.set_render_options()
+
+
 def test_projection_matches_reference_golden():
     z = np.load(GOLDEN / "projection.npz")
     for i in range(4):

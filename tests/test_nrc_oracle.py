@@ -29,7 +29,7 @@ def rand_params(rng, out_scale=0.5):
 
 def test_param_count_matches_the_abi():
     assert N.N_PARAMS == L.NRC_PARAMS == 18624
-    assert L.CACHE_CONFIG.itemsize == 48 and L.CACHE_STATS.itemsize == 32 and L.RENDER_OPTIONS.itemsize == 32
+    assert L.CACHE_CONFIG.itemsize == 48 and L.CACHE_STATS.itemsize == 32 and L.RENDER_OPTIONS.itemsize == 36
 
 
 def test_backward_matches_finite_differences():

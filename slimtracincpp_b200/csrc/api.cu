@@ -61,6 +61,9 @@ struct DevArray {
     void release() { if (ptr) cudaFree(ptr); ptr = nullptr; count = 0; }
 };
 
+// Row bands of a frame in flight at once (queue sets and streams).
+constexpr int kBandLanes = 2;
+
 struct Context {
     bool initialized = false;
     int device = -1;
@@ -91,16 +94,17 @@ struct Context {
     DevScene scene{};
     SlimRenderOptions options{};
     SlimWorkCounters last_counters{};
-    // Queues of the wavefront engine: two sets, so two row bands of a frame
-    // can be in flight at once (one on the caller's stream, one on band_stream).
+    // Queues of the wavefront engine: one set per band lane, so that many
+    // row bands of a frame can be in flight at once (lane 0 on the caller's
+    // stream, the others on band_streams).
     struct WaveSet {
         DevArray<float4> color, through, rays0, rays1, hits, shadow_rays, pairs;
         DevArray<uint32_t> counts;
         DevArray<unsigned long long> mask;
         WavefrontBuffers B{};
-    } wave[2];
-    cudaStream_t band_stream = nullptr;
-    cudaEvent_t band_fork = nullptr, band_join = nullptr;
+    } wave[kBandLanes];
+    cudaStream_t band_streams[kBandLanes] = {};
+    cudaEvent_t band_fork = nullptr, band_join[kBandLanes] = {};
     struct EventTimer *timer = nullptr;
 
     // neural radiance cache
@@ -756,13 +760,14 @@ int read_counters(Context &c, cudaStream_t stream) {
 }
 
 // Row bands of a wavefront frame.  Each band is a complete wavefront pass
-// over its rows; bands alternate between the two queue sets, one on the
-// caller's stream and one on band_stream, so two bands are in flight at
-// once and the ends of one band's persistent launches, where most of the GPU
+// over its rows; bands take the kBandLanes queue sets in turn, the first on
+// the caller's stream and the others on band_streams, so that many bands
+// are in flight at once and the ends of one band's persistent launches, where most of the GPU
 // waits on a few long walks, overlap the other band's work.  Into a pinned
 // host canvas every band downloads as soon as it is done, while the next
 // renders.  The pixels are the same for any band count.
 constexpr uint32_t kDefaultRowBands = 2;
+constexpr double kBandRatio = 2.0 / 3.0;
 constexpr uint32_t kMinBandedSamples = 1u << 18;
 
 uint32_t row_bands(const Context &c, uint32_t sample_rows, uint32_t samples) {
@@ -812,9 +817,12 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     const size_t pix_per_row = ssaa ? (size_t)stride * 2 : stride;
     const size_t dep_per_row = ssaa ? (size_t)stride * 2 : (size_t)stride * (canvas->antialias == SLIM_AA_NONE ? 1 : 4);
     const bool banded_download = download && pinned_host(host_pixels) && pinned_host(host_depths);
-    if (!c.band_stream) SLIM_CUDA(cudaStreamCreateWithFlags(&c.band_stream, cudaStreamNonBlocking), "band stream");
     if (!c.band_fork) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_fork, cudaEventDisableTiming), "band event");
-    if (!c.band_join) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_join, cudaEventDisableTiming), "band event");
+    for (int l = 1; l < kBandLanes; l++) {
+        if (!c.band_streams[l])
+            SLIM_CUDA(cudaStreamCreateWithFlags(&c.band_streams[l], cudaStreamNonBlocking), "band stream");
+        if (!c.band_join[l]) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_join[l], cudaEventDisableTiming), "band event");
+    }
     if (banded_download && !c.copy_stream)
         SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking), "copy stream");
     while (c.band_events.size() < bands + 1) {
@@ -829,14 +837,33 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
                                   stream), "clear counters");
     if ((rc = wait_for_refit(c, stream))) return rc;
     SLIM_CUDA(cudaEventRecord(c.band_fork, stream), "band fork");
-    SLIM_CUDA(cudaStreamWaitEvent(c.band_stream, c.band_fork, 0), "band fork");
-    const cudaStream_t lanes[2] = {stream, c.band_stream};
+    cudaStream_t lanes[kBandLanes];
+    lanes[0] = stream;
+    for (int l = 1; l < kBandLanes; l++) {
+        lanes[l] = c.band_streams[l];
+        SLIM_CUDA(cudaStreamWaitEvent(lanes[l], c.band_fork, 0), "band fork");
+    }
+    // Band b gets a share proportional to kBandRatio^b: unequal bands keep
+    // the two pipelines out of step, so one's launch tails meet the other's
+    // full launches (config 2, two bands: 60/40 1.62 ms, 50/50 1.67 ms).
     const uint32_t tiles = sample_rows / 4;
+    double total = 0.0, w = 1.0;
+    for (uint32_t b = 0; b < bands; b++, w *= kBandRatio) total += w;
+    double cum = 0.0;
+    w = 1.0;
     uint32_t r0 = 0;
-    for (uint32_t b = 0; b < bands; b++) {
-        const uint32_t r1 = b + 1 == bands ? sample_rows : 4 * (uint32_t)((uint64_t)tiles * (b + 1) / bands);
-        const cudaStream_t ls = lanes[b & 1];
-        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, (int)(b & 1))))
+    for (uint32_t b = 0; b < bands; b++, w *= kBandRatio) {
+        cum += w;
+        uint32_t r1 = sample_rows;
+        if (b + 1 < bands) {
+            uint32_t t = (uint32_t)((double)tiles * cum / total);
+            const uint32_t lo = r0 / 4 + 1, hi = tiles - (bands - 1 - b);   // at least one tile band each
+            t = t < lo ? lo : (t > hi ? hi : t);
+            r1 = 4 * t;
+        }
+        const int lane = (int)(b % kBandLanes);
+        const cudaStream_t ls = lanes[lane];
+        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane)))
             return rc;
         if (banded_download) {
             SLIM_CUDA(cudaEventRecord(c.band_events[b], ls), "band event");
@@ -850,8 +877,10 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         }
         r0 = r1;
     }
-    SLIM_CUDA(cudaEventRecord(c.band_join, c.band_stream), "band join");
-    SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join, 0), "band join");
+    for (int l = 1; l < kBandLanes; l++) {
+        SLIM_CUDA(cudaEventRecord(c.band_join[l], lanes[l]), "band join");
+        SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join[l], 0), "band join");
+    }
     if (banded_download) {
         SLIM_CUDA(cudaEventRecord(c.band_events[bands], c.copy_stream), "downloads done");
         SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[bands], 0), "downloads done");

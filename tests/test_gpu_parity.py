@@ -66,8 +66,19 @@ def renderer_for(w, **kw):
                               int(st["skybox_radiance_texture_id"]), int(st["skybox_irradiance_texture_id"]), **kw)
 
 
+def axis_aligned_mesh_scene():
+    """An unrotated camera over an odd-sized canvas: the centre column and row
+    of primary rays have direction components of exactly zero (infinite
+    reciprocals, the slab test's NaN-handling path)."""
+    from slimtracincpp_b200.scene import Camera
+    w = scenes.small_mesh_scene(0, 65, 65)
+    w.camera = Camera(np.eye(3, dtype=np.float32), np.array([0.0, 1.0, -8.0], np.float32), w.camera.focal_length)
+    return w
+
+
 def workloads():
     return {
+        "axis_aligned": axis_aligned_mesh_scene,
         "config1": lambda: scenes.config1(0, 320, 180),
         "config1_seed3": lambda: scenes.config1(3, 256, 144),
         "mesh_small": lambda: scenes.small_mesh_scene(0, 192, 108),

@@ -33,9 +33,7 @@ SLIM_D void world_box(const DevScene &S, uint32_t gi, float mn[3], float mx[3]) 
             }
 }
 
-__global__ void k_refit_leaves(DevScene S, float4 *nodes, uint32_t node_count) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= node_count) return;
+SLIM_D void refit_leaf(const DevScene &S, float4 *nodes, uint32_t i) {
     float4 b = nodes[2 * i + 1];
     uint32_t count = __float_as_uint(b.w) & 0xFFFFu;
     if (!count) return;
@@ -53,12 +51,16 @@ __global__ void k_refit_leaves(DevScene S, float4 *nodes, uint32_t node_count) {
     nodes[2 * i + 1] = make_float4(mx[1], mx[2], b.z, b.w);
 }
 
+__global__ void k_refit_leaves(DevScene S, float4 *nodes, uint32_t node_count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < node_count) refit_leaf(S, nodes, i);
+}
+
 // Inner nodes: `order` lists them by increasing node index and every
 // child pair sits after its parent (checked on upload), so walking the list
 // backwards finishes both children before their parent.  The scene BVH has
 // at most 2 x geometries nodes, so one thread does the whole sweep.
-__global__ void k_refit_inner(float4 *nodes, const uint32_t *order, uint32_t count) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+SLIM_D void refit_inner(float4 *nodes, const uint32_t *order, uint32_t count) {
     for (int32_t k = (int32_t)count - 1; k >= 0; k--) {
         uint32_t i = order[k];
         float4 b = nodes[2 * i + 1];
@@ -70,6 +72,21 @@ __global__ void k_refit_inner(float4 *nodes, const uint32_t *order, uint32_t cou
         nodes[2 * i + 1] = make_float4(mxy, mxz, b.z, b.w);
     }
 }
+__global__ void k_refit_inner(float4 *nodes, const uint32_t *order, uint32_t count) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) refit_inner(nodes, order, count);
+}
+
+// Scenes of up to kRefitBlock nodes: both passes in one block, one launch.
+constexpr uint32_t kRefitBlock = 1024;
+__global__ void __launch_bounds__(kRefitBlock) k_refit_small(DevScene S, float4 *nodes, uint32_t node_count,
+                                                             const uint32_t *order, uint32_t inner_count) {
+    if (threadIdx.x < node_count) refit_leaf(S, nodes, threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence_block();
+        refit_inner(nodes, order, inner_count);
+    }
+}
 
 }  // namespace dev
 
@@ -78,6 +95,13 @@ cudaError_t launch_refit_scene_bvh(const DevScene &S, float4 *scene_nodes, const
     uint32_t n = S.scene_node_count;
     if (!n) return cudaSuccess;
     if (timer) timer->begin(STAGE_REFIT, stream);
+    if (n <= dev::kRefitBlock) {
+        const uint32_t threads = (n + 31) / 32 * 32;
+        dev::k_refit_small<<<1, threads, 0, stream>>>(S, scene_nodes, n, order, inner_count);
+        count_launch();
+        if (timer) timer->end(STAGE_REFIT, stream);
+        return cudaGetLastError();
+    }
     dev::k_refit_leaves<<<(n + 127) / 128, 128, 0, stream>>>(S, scene_nodes, n);
     count_launch();
     if (inner_count) {

@@ -430,33 +430,33 @@ __global__ void __launch_bounds__(256, 4) k_shadow_scene(DevScene S0, DevFrame F
 }
 
 
-// Leaves a walk reaches wait (at most two per lane, in visiting order) while
+// Leaves a walk reaches wait (up to three per lane, in visiting order) while
 // the lane keeps stepping through inner nodes; the warp tests triangles only
 // when most of its lanes have a waiting leaf or none can step, so the
 // triangle code runs with most lanes busy instead of one or two.
 // A lane keeps stepping through inner nodes while at most kStepWhileWaiting
-// leaves wait; the slots hold those plus the two one step can add
-// (config 2: stepping with one leaf waiting 2.03 -> 1.94 ms).
+// leaves wait (config 2: stepping with one leaf waiting 2.03 -> 1.94 ms).
 constexpr uint32_t kStepWhileWaiting = 1;
+// kStepWhileWaiting + 2 slots: a lane steps only with at most
+// kStepWhileWaiting leaves waiting, and a step adds at most two.
 struct PendingLeaves {
-    uint32_t first0, count0, first1, count1, first2, count2, first3, count3;
-    float clip0, clip1, clip2, clip3;
+    uint32_t first0, count0, first1, count1, first2, count2;
+    float clip0, clip1, clip2;
     uint32_t n;
     SLIM_D void push(uint32_t f, uint32_t c, float far) {
         if (n == 0) { first0 = f; count0 = c; clip0 = far; }
         else if (n == 1) { first1 = f; count1 = c; clip1 = far; }
-        else if (n == 2) { first2 = f; count2 = c; clip2 = far; }
-        else { first3 = f; count3 = c; clip3 = far; }
+        else { first2 = f; count2 = c; clip2 = far; }
         n++;
     }
     SLIM_D void pop() {
         first0 = first1; count0 = count1; clip0 = clip1;
         first1 = first2; count1 = count2; clip1 = clip2;
-        first2 = first3; count2 = count3; clip2 = clip3;
         n--;
     }
     SLIM_D bool can_step() const { return n <= kStepWhileWaiting; }
 };
+static_assert(kStepWhileWaiting + 2 <= 3, "PendingLeaves holds three leaves");
 
 // Warp-uniform decision: should idle lanes take new candidates now?  Idle
 // lanes wait until a quarter of the warp is idle (or nobody is busy) and
@@ -478,8 +478,16 @@ SLIM_D bool leaf_round(bool waiting, bool can_step) {
     return wait_mask && (2u * (uint32_t)__popc(wait_mask) >= (uint32_t)__popc(act) || !step_mask);
 }
 
+// The persistent mesh kernels run 128-thread blocks with a register cap
+// that fits one more block per SM than their natural use (shadow: 61 -> 56
+// registers, 32 -> 36 warps per SM; closest hit: 73 -> 70 registers, 24 -> 28
+// warps): their walks wait on dependent loads, so warps beat registers
+// (config 2: 1.61 -> 1.57 ms with the closest-hit pass, 1.59 with the any-hit
+// pass alone).
+constexpr int kMeshBlock = 128;
+
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
     const uint32_t n = *A.pair_count < A.pair_capacity ? *A.pair_count : A.pair_capacity;
     uint32_t stack[kStackCapacity];
     uint32_t err = 0;
@@ -753,7 +761,7 @@ __global__ void __launch_bounds__(256) k_extend_overflow(DevScene S0, DevFrame F
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_extend_mesh(DevScene S, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(kMeshBlock, 7) k_extend_mesh(DevScene S, DevFrame F, QueueArgs A) {
     const uint32_t cap = A.pair_capacity * 3u / 4u;
     const uint32_t n = *A.pair_count < cap ? *A.pair_count : cap;
     uint32_t stack[kStackCapacity];
@@ -1261,7 +1269,10 @@ struct RoundLaunch {
     bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
     unsigned long long *stage(int st) const { return counters ? counters + kCountersPerStage * st : nullptr; }
-    uint32_t grid(const void *kernel, uint32_t work) const {
+    uint32_t grid(const void *kernel, uint32_t work) const { return grid_for(kernel, work, block); }
+    // the persistent mesh kernels run 128-thread blocks (kMeshBlock)
+    uint32_t mesh_grid(const void *kernel, uint32_t work) const { return grid_for(kernel, work, kMeshBlock); }
+    uint32_t grid_for(const void *kernel, uint32_t work, int block) const {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
         if (share_sms && per_sm > 1) per_sm--;
@@ -1323,7 +1334,8 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (r != cudaSuccess) return r;
         k_extend_scene<COUNT, BATCH><<<L.grid((const void *)k_extend_scene<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
         count_launch();
-        k_extend_mesh<COUNT><<<L.grid((const void *)k_extend_mesh<COUNT>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
+        k_extend_mesh<COUNT><<<L.mesh_grid((const void *)k_extend_mesh<COUNT>, B.pair_capacity), kMeshBlock, 0,
+                               stream>>>(S, F, A);
         count_launch();
         k_extend_resolve<COUNT, BATCH><<<L.grid((const void *)k_extend_resolve<COUNT, BATCH>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
         count_launch();
@@ -1367,7 +1379,8 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (timer) timer->end(STAGE_SHADOW, stream);
         A.counters = L.stage(STAGE_SHADOW_MESH);
         if (timer) timer->begin(STAGE_SHADOW_MESH, stream);
-        k_shadow_mesh<COUNT><<<L.grid((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), L.block, 0, stream>>>(S, F, A);
+        k_shadow_mesh<COUNT><<<L.mesh_grid((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), kMeshBlock, 0,
+                               stream>>>(S, F, A);
         count_launch();
         if (timer) timer->end(STAGE_SHADOW_MESH, stream);
     }

@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--config", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
                    help="workload (default: config2, the metric's 1080p mesh PBR scene)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--row-bands", type=int, default=0,
+                   help="row bands of every wavefront frame (0: the library default; 1: whole frames, as for ncu "
+                        "captures of whole-frame launches)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     return p.parse_args()
 
@@ -201,7 +204,7 @@ def algorithmic_bytes(w, pixels=None):
 # these are cold-cache bytes.  A stage launch is all kernels of one round: extend = scene + mesh + resolve + overflow.
 TRAFFIC_BYTES_PER_LAUNCH = {
     ("config2", "extend"): 180.0e6,       # rounds 1 and 2: 259 MB and 101 MB
-    ("config2", "shadow_mesh"): 61.7e6,   # 92.9 MB and 29.9 MB
+    ("config2", "shadow_mesh"): 61.6e6,   # 93.0 MB and 30.2 MB
 }
 PIXEL_STAGES = ("shade", "tail", "fused")   # stages that write the framebuffer
 
@@ -623,7 +626,7 @@ def main():
     r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
     torch.cuda.synchronize()
     work = native.work_counters()
-    native.set_render_options(engine=engine, count_work=True, profile_stages=True)
+    native.set_render_options(engine=engine, count_work=True, profile_stages=True, row_bands=args.row_bands)
     native.reset_stage_stats()
     native.check(lib.slimRefitSceneBVH(sp))
     r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr(), sp)
@@ -635,7 +638,7 @@ def main():
 
     # timed device-resident frames: the library's default frame (row bands
     # in flight on two streams), no per-stage events in the way
-    native.set_render_options(engine=engine)
+    native.set_render_options(engine=engine, row_bands=args.row_bands)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
         native.check(lib.slimRefitSceneBVH(sp))
@@ -676,7 +679,7 @@ def main():
     stats = {s["name"]: s for s in native.stage_stats()}
 
     # end to end through the C ABI with host buffers
-    native.set_render_options(engine=engine)
+    native.set_render_options(engine=engine, row_bands=args.row_bands)
     pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
     pin_geo = torch.empty(w.scene.geometries.nbytes, dtype=torch.uint8, pin_memory=True)
@@ -736,7 +739,7 @@ def main():
                        "triangles": sum(m.triangle_count for m in w.scene.meshes),
                        "textures": len(w.scene.textures), "lights": len(w.scene.lights),
                        "engine": args.engine, "parallelism": f"replicas x{world}",
-                       "row_bands": (2 if n >= 1 << 18 else 1) if args.engine == "wavefront" else 1,
+                       "row_bands": (args.row_bands or (2 if n >= 1 << 18 else 1)) if args.engine == "wavefront" else 1,
                        "l2": "flushed between steps (512 MiB write)", "rays_per_frame": rays_per_frame,
                        "primary_rays": work["primary_rays"], "shadow_rays": work["shadow_rays"],
                        "bounce_rays": work["bounce_rays"]},

@@ -632,7 +632,7 @@ int wait_for_refit(Context &c, cudaStream_t stream) {
 // frame).
 int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
            const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream,
-           uint32_t row_begin, uint32_t rows, bool first, int set = 0) {
+           uint32_t row_begin, uint32_t rows, bool first, int set = 0, const FrameDownload *download = nullptr) {
     const SlimDimensions &dim = canvas->dimensions;
     if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
     if (canvas->antialias < SLIM_AA_NONE || canvas->antialias > SLIM_AA_SSAA) return set_error(SLIM_ERR_ARGUMENT, "bad antialias mode");
@@ -674,7 +674,7 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
             if ((rc = cache_frame(c, F.width * F.rows, cf))) return rc;
             cache = &cf;
         }
-        e = launch_render_wavefront(c.scene, F, c.wave[set].B, c.options.block_size, stream, timer, cache);
+        e = launch_render_wavefront(c.scene, F, c.wave[set].B, c.options.block_size, stream, timer, cache, download);
     }
     if (e != cudaSuccess) return cuda_fail(e, "render launch");
     return SLIM_OK;
@@ -779,6 +779,18 @@ uint32_t row_bands(const Context &c, uint32_t sample_rows, uint32_t samples) {
     return bands;
 }
 
+// The device's address of pinned host memory mapped into its address space.
+bool mapped_host(const void *p, void **device_address) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return false;
+    *device_address = a.devicePointer;
+    return true;
+}
+
 bool pinned_host(const void *p) {
     cudaPointerAttributes a{};
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -817,6 +829,14 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     const size_t pix_per_row = ssaa ? (size_t)stride * 2 : stride;
     const size_t dep_per_row = ssaa ? (size_t)stride * 2 : (size_t)stride * (canvas->antialias == SLIM_AA_NONE ? 1 : 4);
     const bool banded_download = download && pinned_host(host_pixels) && pinned_host(host_depths);
+    // Pinned canvases the device can address: each band's rows download as
+    // soon as its first round is done, and later pixels go straight there.
+    float4 *mapped_pixels = nullptr;
+    float *mapped_depths = nullptr;
+    const bool early = banded_download && c.options.engine == SLIM_ENGINE_WAVEFRONT &&
+                       c.options.radiance_cache == SLIM_CACHE_OFF && settings->render_mode == SLIM_RENDER_BEAUTY &&
+                       settings->max_depth >= 1 && mapped_host(host_pixels, (void **)&mapped_pixels) &&
+                       mapped_host(host_depths, (void **)&mapped_depths);
     if (!c.band_fork) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_fork, cudaEventDisableTiming), "band event");
     for (int l = 1; l < kBandLanes; l++) {
         if (!c.band_streams[l])
@@ -825,7 +845,7 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     }
     if (banded_download && !c.copy_stream)
         SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking), "copy stream");
-    while (c.band_events.size() < bands + 1) {
+    while (c.band_events.size() < 2 * bands + 1) {
         cudaEvent_t e;
         SLIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
         c.band_events.push_back(e);
@@ -863,13 +883,31 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         }
         const int lane = (int)(b % kBandLanes);
         const cudaStream_t ls = lanes[lane];
+        const size_t p0 = pix_per_row * r0, pn = pix_per_row * (r1 - r0);
+        const size_t d0 = dep_per_row * r0, dn = dep_per_row * (r1 - r0);
+        if (early) {
+            FrameDownload dl{};
+            dl.copy_stream = c.copy_stream;
+            dl.round_done = c.band_events[2 * b];
+            dl.copied = c.band_events[2 * b + 1];
+            dl.host_pixels = host_pixels + p0;
+            dl.host_depths = host_depths + d0;
+            dl.dev_pixels = d_pixels + p0;
+            dl.dev_depths = d_depths + d0;
+            dl.pixel_bytes = pn * sizeof(float4);
+            dl.depth_bytes = dn * sizeof(float);
+            dl.mapped_pixels = mapped_pixels;
+            dl.mapped_depths = mapped_depths;
+            if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane, &dl)))
+                return rc;
+            r0 = r1;
+            continue;
+        }
         if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane)))
             return rc;
         if (banded_download) {
             SLIM_CUDA(cudaEventRecord(c.band_events[b], ls), "band event");
             SLIM_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_events[b], 0), "band wait");
-            const size_t p0 = pix_per_row * r0, pn = pix_per_row * (r1 - r0);
-            const size_t d0 = dep_per_row * r0, dn = dep_per_row * (r1 - r0);
             SLIM_CUDA(cudaMemcpyAsync(host_pixels + p0, d_pixels + p0, pn * sizeof(float4), cudaMemcpyDeviceToHost,
                                       c.copy_stream), "download pixels");
             SLIM_CUDA(cudaMemcpyAsync(host_depths + d0, d_depths + d0, dn * sizeof(float), cudaMemcpyDeviceToHost,
@@ -882,8 +920,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join[l], 0), "band join");
     }
     if (banded_download) {
-        SLIM_CUDA(cudaEventRecord(c.band_events[bands], c.copy_stream), "downloads done");
-        SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[bands], 0), "downloads done");
+        SLIM_CUDA(cudaEventRecord(c.band_events[2 * bands], c.copy_stream), "downloads done");
+        SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[2 * bands], 0), "downloads done");
     } else if (download) {
         SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, stream),
                   "download pixels");

@@ -90,8 +90,25 @@ struct CacheFrame {
                                               // (what the queries read) once per frame
 };
 
+// Download of a frame's (or band's) canvas rows while its later bounces
+// still run (no counterpart in the reference).  After the first round every
+// path that ends at its first hit has its pixel, so the rows are copied to
+// the host then, on copy_stream; the later rounds write the pixels they
+// finish straight into the host canvas (pinned and mapped into the device's
+// address space), once the copy has landed.
+struct FrameDownload {
+    cudaStream_t copy_stream;
+    cudaEvent_t round_done, copied;       // recorded by the launcher
+    void *host_pixels, *host_depths;      // destinations of the copies
+    const void *dev_pixels, *dev_depths;  // sources of the copies
+    size_t pixel_bytes, depth_bytes;
+    float4 *mapped_pixels;                // the whole host canvas, as the device sees it
+    float *mapped_depths;
+};
+
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache = nullptr);
+                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache = nullptr,
+                                    const FrameDownload *download = nullptr);
 
 // Batched requests (no counterpart in the reference): many requests, each
 // with its own scene, camera and canvas, traced together over one set of

@@ -1268,6 +1268,7 @@ struct RoundLaunch {
     uint32_t lights;     // most lights of any scene in the round
     bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
+    cudaEvent_t pixel_wait = nullptr;  // kernels that write pixels wait for it (a download in flight)
     unsigned long long *stage(int st) const { return counters ? counters + kCountersPerStage * st : nullptr; }
     uint32_t grid(const void *kernel, uint32_t work) const { return grid_for(kernel, work, block); }
     // the persistent mesh kernels run 128-thread blocks (kMeshBlock)
@@ -1298,6 +1299,10 @@ cudaError_t tail_round(const RoundLaunch &L, QueueArgs &A, uint32_t in, uint32_t
     A.depth = depth;
     A.rays_in = B.rays[in];
     A.count_in = B.queue_count + in;
+    if (L.pixel_wait) {
+        cudaError_t r = cudaStreamWaitEvent(L.stream, L.pixel_wait, 0);
+        if (r != cudaSuccess) return r;
+    }
     A.counters = L.stage(STAGE_TAIL);
     if (L.timer) L.timer->begin(STAGE_TAIL, L.stream);
     RoundLaunch T = L;
@@ -1384,6 +1389,7 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         count_launch();
         if (timer) timer->end(STAGE_SHADOW_MESH, stream);
     }
+    if (L.pixel_wait && (r = cudaStreamWaitEvent(stream, L.pixel_wait, 0)) != cudaSuccess) return r;
     A.counters = L.stage(STAGE_SHADE);
     if (timer) timer->begin(STAGE_SHADE, stream);
     k_shade<COUNT, BATCH><<<L.grid((const void *)k_shade<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
@@ -1522,7 +1528,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
 
 template <bool COUNT>
 cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block, cudaStream_t stream,
-                      StageTimer *timer, const CacheFrame *cache) {
+                      StageTimer *timer, const CacheFrame *cache, const FrameDownload *dl) {
     uint32_t samples = F.width * F.rows;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1554,6 +1560,7 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     if (use_cache && (e = cudaMemsetAsync(cache->counts, 0, sizeof(uint32_t), stream)) != cudaSuccess) return e;
     uint32_t in = 0;
     const uint32_t last = use_cache ? cache->depth : max_depth;
+    DevFrame late = F;   // the frame as the rounds after a download see it
     for (uint32_t depth = 1; depth <= last; depth++) {
         if (!L.split_extend && depth >= kTailDepth && !(use_cache && depth == last)) {
             if ((e = tail_round<COUNT, false>(L, A, in, depth)) != cudaSuccess) return e;
@@ -1561,6 +1568,23 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
         }
         if ((e = trace_round<COUNT, false>(L, A, CA, in, depth, depth == 1, use_cache && depth == last)) != cudaSuccess)
             return e;
+        if (depth == 1 && dl && !use_cache) {
+            // every path that ended at its first hit has written its pixel:
+            // the rows go to the host now; later pixels go there directly
+            if ((e = cudaEventRecord(dl->round_done, stream)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(dl->copy_stream, dl->round_done, 0)) != cudaSuccess) return e;
+            if ((e = cudaMemcpyAsync(dl->host_pixels, dl->dev_pixels, dl->pixel_bytes, cudaMemcpyDeviceToHost,
+                                     dl->copy_stream)) != cudaSuccess)
+                return e;
+            if ((e = cudaMemcpyAsync(dl->host_depths, dl->dev_depths, dl->depth_bytes, cudaMemcpyDeviceToHost,
+                                     dl->copy_stream)) != cudaSuccess)
+                return e;
+            if ((e = cudaEventRecord(dl->copied, dl->copy_stream)) != cudaSuccess) return e;
+            late.pixels = dl->mapped_pixels;
+            late.depths = dl->mapped_depths;
+            L.F = &late;
+            L.pixel_wait = dl->copied;
+        }
     }
     if (!use_cache) return cudaSuccess;
     A.cache = CA;
@@ -1624,12 +1648,13 @@ cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block
 }  // namespace dev
 
 cudaError_t launch_render_wavefront(const DevScene &S, const DevFrame &F, const WavefrontBuffers &B, int block,
-                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache) {
+                                    cudaStream_t stream, StageTimer *timer, const CacheFrame *cache,
+                                    const FrameDownload *download) {
     if (F.settings.render_mode != SLIM_RENDER_BEAUTY)   // a single primary hit: nothing to queue
         return launch_render_fused(S, F, block, stream, timer);
     if (F.settings.max_depth == 0) return launch_render_fused(S, F, block, stream, timer);
-    if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer, cache);
-    return dev::run_frame<false>(S, F, B, block, stream, timer, cache);
+    if (F.counters) return dev::run_frame<true>(S, F, B, block, stream, timer, cache, download);
+    return dev::run_frame<false>(S, F, B, block, stream, timer, cache, download);
 }
 
 cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,

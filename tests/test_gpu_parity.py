@@ -237,16 +237,24 @@ def test_pick_selects_a_light_in_front_of_the_geometry():
     assert int(far["light"]) == -1
 
 
+BANDED_SCENES = {
+    "mesh_depth2": lambda: scenes.small_mesh_scene(0, 120, 70),
+    "implicit_depth6": lambda: scenes.feature_scene(4, 120, 70, max_depth=6),   # late bounces in the fused tail
+}
+
+
 @pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("antialias", [L.AA_NONE, L.AA_MSAA, L.AA_SSAA])
-def test_banded_download_into_a_pinned_canvas(engine, antialias):
+@pytest.mark.parametrize("scene", list(BANDED_SCENES))
+def test_banded_download_into_a_pinned_canvas(engine, antialias, scene):
     """slimRenderOnGPU renders the frame in row bands, two in flight on two
-    streams, and into pinned host memory downloads each band while the next
-    renders: the canvas must equal the one-band frame bit for bit, for any
-    band count (70 rows: the last band also holds the rows past the last
-    4-row tile band)."""
+    streams.  Into pinned host memory each band's rows download once its
+    first round is done, and the pixels of later bounces are written into the
+    host canvas directly: the canvas must equal the one-band frame bit for
+    bit, for any band count (70 rows: the last band also holds the rows past
+    the last 4-row tile band)."""
     from slimtracincpp_b200.renderer import make_canvas
-    w = scenes.small_mesh_scene(0, 120, 70)
+    w = BANDED_SCENES[scene]()
     r = renderer_for(w)
     vp = Viewport(w.camera, w.width, w.height, antialias)
     native.set_render_options(engine=engine)

@@ -68,7 +68,7 @@ struct Context {
     bool initialized = false;
     int device = -1;
     cudaStream_t stream = nullptr;
-    cudaStream_t copy_stream = nullptr;          // banded downloads
+    cudaStream_t copy_streams[kBandLanes] = {};  // banded downloads, one per band lane
     cudaEvent_t refit_done = nullptr;            // the last scene BVH refit, on the caller's stream
     std::vector<cudaEvent_t> band_events;        // one per band, the last marks the downloads' end
     SlimSceneCounts counts{};
@@ -843,9 +843,12 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
             SLIM_CUDA(cudaStreamCreateWithFlags(&c.band_streams[l], cudaStreamNonBlocking), "band stream");
         if (!c.band_join[l]) SLIM_CUDA(cudaEventCreateWithFlags(&c.band_join[l], cudaEventDisableTiming), "band event");
     }
-    if (banded_download && !c.copy_stream)
-        SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking), "copy stream");
-    while (c.band_events.size() < 2 * bands + 1) {
+    // one copy stream per lane: a band's copy waits for its own band only,
+    // not for a band on another lane that finishes later
+    for (int l = 0; banded_download && l < kBandLanes; l++)
+        if (!c.copy_streams[l])
+            SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_streams[l], cudaStreamNonBlocking), "copy stream");
+    while (c.band_events.size() < 2 * bands + kBandLanes) {
         cudaEvent_t e;
         SLIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
         c.band_events.push_back(e);
@@ -887,7 +890,7 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         const size_t d0 = dep_per_row * r0, dn = dep_per_row * (r1 - r0);
         if (early) {
             FrameDownload dl{};
-            dl.copy_stream = c.copy_stream;
+            dl.copy_stream = c.copy_streams[lane];
             dl.round_done = c.band_events[2 * b];
             dl.copied = c.band_events[2 * b + 1];
             dl.host_pixels = host_pixels + p0;
@@ -907,11 +910,11 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
             return rc;
         if (banded_download) {
             SLIM_CUDA(cudaEventRecord(c.band_events[b], ls), "band event");
-            SLIM_CUDA(cudaStreamWaitEvent(c.copy_stream, c.band_events[b], 0), "band wait");
+            SLIM_CUDA(cudaStreamWaitEvent(c.copy_streams[lane], c.band_events[b], 0), "band wait");
             SLIM_CUDA(cudaMemcpyAsync(host_pixels + p0, d_pixels + p0, pn * sizeof(float4), cudaMemcpyDeviceToHost,
-                                      c.copy_stream), "download pixels");
+                                      c.copy_streams[lane]), "download pixels");
             SLIM_CUDA(cudaMemcpyAsync(host_depths + d0, d_depths + d0, dn * sizeof(float), cudaMemcpyDeviceToHost,
-                                      c.copy_stream), "download depths");
+                                      c.copy_streams[lane]), "download depths");
         }
         r0 = r1;
     }
@@ -920,8 +923,10 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join[l], 0), "band join");
     }
     if (banded_download) {
-        SLIM_CUDA(cudaEventRecord(c.band_events[2 * bands], c.copy_stream), "downloads done");
-        SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[2 * bands], 0), "downloads done");
+        for (int l = 0; l < kBandLanes; l++) {
+            SLIM_CUDA(cudaEventRecord(c.band_events[2 * bands + l], c.copy_streams[l]), "downloads done");
+            SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[2 * bands + l], 0), "downloads done");
+        }
     } else if (download) {
         SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, stream),
                   "download pixels");

@@ -2,12 +2,15 @@
 // plus the device-resident extensions.  One process-wide render context,
 // like the reference's module-global GPU mirror (renderer/renderer_GPU.h:
 // 12-20); calls are serialised by a mutex.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -64,11 +67,96 @@ struct DevArray {
 // Row bands of a frame in flight at once (queue sets and streams).
 constexpr int kBandLanes = 2;
 
+// Host threads that copy a finished frame from the pinned staging canvas
+// into a pageable one: the driver's own download into pageable memory runs
+// at about a third of the PCIe rate, one core copying from its bounce
+// buffers.
+class HostCopyPool {
+  public:
+    ~HostCopyPool() {
+        {
+            std::lock_guard<std::mutex> lock(m_);
+            stop_ = true;
+        }
+        start_.notify_all();
+        for (std::thread &t : threads_) t.join();
+    }
+    // dst[0, bytes) = src[0, bytes), split over the pool; returns when done.
+    void copy(void *dst, const void *src, size_t bytes) {
+        if (bytes < kChunk) {
+            memcpy(dst, src, bytes);
+            return;
+        }
+        std::unique_lock<std::mutex> lock(m_);
+        if (threads_.empty()) {
+            unsigned n = std::thread::hardware_concurrency();
+            n = n < 2 ? 2 : (n > 16 ? 16 : n);
+            for (unsigned i = 0; i < n; i++) threads_.emplace_back([this] { work(); });
+        }
+        dst_ = (char *)dst;
+        src_ = (const char *)src;
+        bytes_ = bytes;
+        next_ = 0;
+        busy_ = (uint32_t)threads_.size();
+        generation_++;
+        start_.notify_all();
+        done_.wait(lock, [this] { return busy_ == 0; });
+    }
+
+  private:
+    static constexpr size_t kChunk = 1 << 20;
+    void work() {
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lock(m_);
+            start_.wait(lock, [&] { return stop_ || generation_ != seen; });
+            if (stop_) return;
+            seen = generation_;
+            for (;;) {
+                const size_t off = next_;
+                if (off >= bytes_) break;
+                next_ = off + kChunk;
+                const size_t n = std::min(kChunk, bytes_ - off);
+                lock.unlock();
+                memcpy(dst_ + off, src_ + off, n);
+                lock.lock();
+            }
+            if (--busy_ == 0) done_.notify_one();
+        }
+    }
+    std::mutex m_;
+    std::condition_variable start_, done_;
+    std::vector<std::thread> threads_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0, next_ = 0;
+    uint32_t busy_ = 0;
+    uint64_t generation_ = 0;
+    bool stop_ = false;
+};
+
+// Pinned, device-mapped host memory.
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaHostAlloc(&ptr, n, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+};
+
 struct Context {
     bool initialized = false;
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_streams[kBandLanes] = {};  // banded downloads, one per band lane
+    PinnedBuffer stage_pixels, stage_depths;     // pageable canvases: the frame lands here first
+    HostCopyPool copy_pool;
     cudaEvent_t refit_done = nullptr;            // the last scene BVH refit, on the caller's stream
     std::vector<cudaEvent_t> band_events;        // one per band, the last marks the downloads' end
     SlimSceneCounts counts{};
@@ -389,6 +477,12 @@ int upload_meshes(Context &c, const SlimSceneData *s) {
         memset(&dm, 0, sizeof(dm));
         dm.aabb_min[0] = m.aabb.min.x; dm.aabb_min[1] = m.aabb.min.y; dm.aabb_min[2] = m.aabb.min.z;
         dm.aabb_max[0] = m.aabb.max.x; dm.aabb_max[1] = m.aabb.max.y; dm.aabb_max[2] = m.aabb.max.z;
+        // The reference's builder lays a mesh BVH out as the root followed by
+        // child pairs, so every pair starts at an odd node index: an odd
+        // absolute root index puts every pair on a 64-byte boundary and no
+        // pair straddles two 128-byte cache lines (at most one node of
+        // padding per mesh).
+        if (total_nodes % 2 == 0) total_nodes++;
         dm.node_offset = (uint32_t)total_nodes;
         dm.tri_offset = (uint32_t)total_tris;
         dm.tri_count = m.triangle_count;
@@ -767,6 +861,7 @@ int read_counters(Context &c, cudaStream_t stream) {
 // host canvas every band downloads as soon as it is done, while the next
 // renders.  The pixels are the same for any band count.
 constexpr uint32_t kDefaultRowBands = 2;
+constexpr size_t kStagedDownloadBytes = 4u << 20;   // pageable canvases from here up go through staging
 constexpr double kBandRatio = 2.0 / 3.0;
 constexpr uint32_t kMinBandedSamples = 1u << 18;
 
@@ -1033,10 +1128,27 @@ int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection 
     int rc = c.d_pixels.reserve(pixel_count, "alloc frame");
     if (rc) return rc;
     if ((rc = c.d_depths.reserve(depth_count, "alloc depths"))) return rc;
-    if ((rc = render_frame(c, canvas, projection, settings, c.d_pixels.ptr, c.d_depths.ptr, c.stream, canvas->pixels,
-                           canvas->depths, pixel_count, depth_count)))
+    // A pageable canvas of a large frame: the frame downloads into pinned
+    // staging (banded, while it renders), then host threads copy it over.
+    SlimPixel *host_pixels = canvas->pixels;
+    float *host_depths = canvas->depths;
+    const size_t pixel_bytes = pixel_count * sizeof(float4), depth_bytes = depth_count * sizeof(float);
+    const bool staged = pixel_bytes >= kStagedDownloadBytes &&
+                        !(pinned_host(canvas->pixels) && pinned_host(canvas->depths));
+    if (staged) {
+        SLIM_CUDA(c.stage_pixels.reserve(pixel_bytes), "pinned staging");
+        SLIM_CUDA(c.stage_depths.reserve(depth_bytes), "pinned staging");
+        host_pixels = (SlimPixel *)c.stage_pixels.ptr;
+        host_depths = (float *)c.stage_depths.ptr;
+    }
+    if ((rc = render_frame(c, canvas, projection, settings, c.d_pixels.ptr, c.d_depths.ptr, c.stream, host_pixels,
+                           host_depths, pixel_count, depth_count)))
         return rc;
     if ((rc = read_errors(c, c.stream))) return rc;
+    if (staged) {
+        c.copy_pool.copy(canvas->pixels, host_pixels, pixel_bytes);
+        c.copy_pool.copy(canvas->depths, host_depths, depth_bytes);
+    }
     return read_counters(c, c.stream);
 }
 

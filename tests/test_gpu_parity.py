@@ -308,3 +308,22 @@ def test_row_bands_on_the_callers_stream_with_work_counters():
             assert work[k] == ref[k], k
         for k in ("mesh_node_tests", "triangle_tests"):
             assert abs(work[k] - ref[k]) <= 0.02 * ref[k], k
+
+
+def test_pageable_canvas_through_pinned_staging():
+    """A pageable canvas of at least 4 MB of pixels: the frame downloads into
+    the library's pinned staging canvas (banded, early) and host threads copy
+    it over; the pixels equal the device-resident frame bit for bit."""
+    w = scenes.small_mesh_scene(2, 640, 480)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    n = w.width * w.height
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    pix, dep = r.render(vp)                  # numpy arrays: pageable
+    assert pix.nbytes >= 4 << 20
+    d_pix = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    d_dep = torch.zeros(n, dtype=torch.float32, device="cuda")
+    r.render_to_device(vp, d_pix.data_ptr(), d_dep.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(pix.view(np.uint32), d_pix.cpu().numpy().view(np.uint32))
+    assert np.array_equal(dep.view(np.uint32), d_dep.cpu().numpy().view(np.uint32))

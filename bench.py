@@ -207,6 +207,7 @@ TRAFFIC_BYTES_PER_LAUNCH = {
     ("config2", "shadow_mesh"): 61.6e6,   # 93.0 MB and 30.2 MB
 }
 PIXEL_STAGES = ("shade", "tail", "fused")   # stages that write the framebuffer
+CACHE_WARMUP_FRAMES = 16   # radiance-cache frames trained before the timed ones
 
 
 def measured_peaks():
@@ -364,7 +365,10 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     cache = RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=args.seed)
     native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True, radiance_cache=L.CACHE_ON)
     outs = buffers(steps)
-    for _ in range(args.warmup):
+    # the cache learns online: its first frames are its warm-up (at least
+    # CACHE_WARMUP_FRAMES frames, or the bench's warm-up count if larger)
+    cache_warmup = max(args.warmup, CACHE_WARMUP_FRAMES)
+    for _ in range(cache_warmup):
         native.check(lib.slimRefitSceneBVH(sp))
         r.render_to_device(vp, outs[0][0].data_ptr(), outs[0][1].data_ptr(), sp)
     cache.join(sp)
@@ -447,6 +451,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
             "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded config2 scene, depth 8)",
             "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 8, "cache_depth": 2,
                        "train_samples_per_frame": 65536, "batch": 16384, "learning_rate": 1e-2,
+                       "cache_warmup_frames": cache_warmup,
                        "engine": "wavefront", "parallelism": f"replicas x{world}",
                        "l2": "flushed between steps (512 MiB write)", "rays_per_frame": cache_rays},
             "ms_per_frame": cache_total / steps,

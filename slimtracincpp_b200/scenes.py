@@ -439,8 +439,8 @@ def small_textured_scene(seed=0, width=160, height=90, max_depth=8):
 
 def config4(seed=0, width=1920, height=1080, meshes=None):
     """The radiance-cache workload: config 2's scene with bounce depth 8 (the
-    plain depth-8 frame is the judge of the cache frame, whose paths stop at
-    vertex 2 and take the cache's answer)."""
+    plain depth-8 frame is the reference image for the cache frame, whose
+    paths stop at vertex 2 and take the cache's answer)."""
     w = config2(seed, width, height, meshes)
     w.name = f"config4_cache_mesh_pbr_{width}x{height}_d8_cache2"
     w.settings = L.default_settings(max_depth=8)

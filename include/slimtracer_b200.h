@@ -262,7 +262,10 @@ int slimUploadSceneBVH(const SlimSceneData *scene);
 /* Replaces renderOnGPU(const Canvas&, const CameraRayProjection&,
  * const RayTracerSettings&) (renderer/renderer_GPU.h:148-168): traces every
  * pixel (every sub-sample under SSAA) and writes canvas->pixels (Pixel
- * {clamp(c)^2, 1}) and canvas->depths synchronously, like the reference. */
+ * {clamp(c)^2, 1}) and canvas->depths synchronously, like the reference.
+ * Into pinned host memory (cudaHostAlloc) the rows download while later
+ * bounces still render; a pageable canvas of 4 MB of pixels or more goes
+ * through the library's own pinned staging buffer and a host copy. */
 int slimRenderOnGPU(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
                     const SlimRayTracerSettings *settings);
 

@@ -1627,11 +1627,16 @@ struct BatchState {
     uint32_t max_lights = 0, max_instances = 0;
     bool any_cache = false;
     SlimBatchPlan plan{};
-    // queues of a wave
-    DevArray<float4> color, through, rays0, rays1, hits, shadow_rays, pairs;
-    DevArray<uint32_t> counts;
-    DevArray<unsigned long long> masks;
-    WavefrontBuffers B{};
+    // queues of a wave, one set per wave lane (waves alternate between the
+    // launching stream and lane_stream)
+    struct Queues {
+        DevArray<float4> color, through, rays0, rays1, hits, shadow_rays, pairs;
+        DevArray<uint32_t> counts;
+        DevArray<unsigned long long> masks;
+        WavefrontBuffers B{};
+    } q[2];
+    cudaStream_t lane_stream = nullptr;
+    cudaEvent_t lane_fork = nullptr, lane_join = nullptr;
     // cache queries of a wave (the batch's own buffers, so single frames never
     // move what a captured batch graph points at)
     CacheFrame cache{};
@@ -1717,28 +1722,33 @@ int ensure_batch_queues(BatchState &b) {
     size_t pairs = shadow * inst, max_pairs = budget / (3 * sizeof(float4));
     if (pairs > max_pairs) pairs = max_pairs;
     int rc;
-    if ((rc = b.color.reserve(Q, "alloc batch paths"))) return rc;
-    if ((rc = b.through.reserve(Q, "alloc batch paths"))) return rc;
-    if ((rc = b.rays0.reserve(2 * Q, "alloc batch rays"))) return rc;
-    if ((rc = b.rays1.reserve(2 * Q, "alloc batch rays"))) return rc;
-    if ((rc = b.hits.reserve(3 * Q, "alloc batch hits"))) return rc;
-    if ((rc = b.shadow_rays.reserve(2 * shadow, "alloc batch shadow rays"))) return rc;
-    if ((rc = b.pairs.reserve(3 * pairs, "alloc batch shadow pairs"))) return rc;
-    if ((rc = b.counts.reserve(8, "alloc batch counters"))) return rc;
-    if ((rc = b.masks.reserve(Q, "alloc batch masks"))) return rc;
-    WavefrontBuffers &B = b.B;
-    B.path_color = b.color.ptr;
-    B.path_throughput = b.through.ptr;
-    B.rays[0] = b.rays0.ptr;
-    B.rays[1] = b.rays1.ptr;
-    B.queue_count = b.counts.ptr;
-    B.hits = b.hits.ptr;
-    B.shadow_rays = b.shadow_rays.ptr;
-    B.shadow_mask = b.masks.ptr;
-    B.pairs = b.pairs.ptr;
-    B.capacity = (uint32_t)Q;
-    B.shadow_capacity = (uint32_t)shadow;
-    B.pair_capacity = (uint32_t)pairs;
+    for (BatchState::Queues &u : b.q) {
+        if ((rc = u.color.reserve(Q, "alloc batch paths"))) return rc;
+        if ((rc = u.through.reserve(Q, "alloc batch paths"))) return rc;
+        if ((rc = u.rays0.reserve(2 * Q, "alloc batch rays"))) return rc;
+        if ((rc = u.rays1.reserve(2 * Q, "alloc batch rays"))) return rc;
+        if ((rc = u.hits.reserve(3 * Q, "alloc batch hits"))) return rc;
+        if ((rc = u.shadow_rays.reserve(2 * shadow, "alloc batch shadow rays"))) return rc;
+        if ((rc = u.pairs.reserve(3 * pairs, "alloc batch shadow pairs"))) return rc;
+        if ((rc = u.counts.reserve(8, "alloc batch counters"))) return rc;
+        if ((rc = u.masks.reserve(Q, "alloc batch masks"))) return rc;
+        WavefrontBuffers &B = u.B;
+        B.path_color = u.color.ptr;
+        B.path_throughput = u.through.ptr;
+        B.rays[0] = u.rays0.ptr;
+        B.rays[1] = u.rays1.ptr;
+        B.queue_count = u.counts.ptr;
+        B.hits = u.hits.ptr;
+        B.shadow_rays = u.shadow_rays.ptr;
+        B.shadow_mask = u.masks.ptr;
+        B.pairs = u.pairs.ptr;
+        B.capacity = (uint32_t)Q;
+        B.shadow_capacity = (uint32_t)shadow;
+        B.pair_capacity = (uint32_t)pairs;
+    }
+    if (!b.lane_stream) SLIM_CUDA(cudaStreamCreateWithFlags(&b.lane_stream, cudaStreamNonBlocking), "batch lane stream");
+    if (!b.lane_fork) SLIM_CUDA(cudaEventCreateWithFlags(&b.lane_fork, cudaEventDisableTiming), "batch lane event");
+    if (!b.lane_join) SLIM_CUDA(cudaEventCreateWithFlags(&b.lane_join, cudaEventDisableTiming), "batch lane event");
     return SLIM_OK;
 }
 
@@ -1794,7 +1804,11 @@ int batch_launch(Context &c, BatchState &b, cudaStream_t stream) {
     BF.waves = b.waves.data();
     BF.wave_count = (uint32_t)b.waves.size();
     BF.cache = b.any_cache ? &b.cache : nullptr;
-    cudaError_t e = launch_render_batch(BF, b.B, b.plan.block_size, stream, nullptr);
+    BF.lane_stream = b.lane_stream;
+    BF.lane_queues = &b.q[1].B;
+    BF.lane_fork = b.lane_fork;
+    BF.lane_join = b.lane_join;
+    cudaError_t e = launch_render_batch(BF, b.q[0].B, b.plan.block_size, stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "batch launch");
     return SLIM_OK;
 }

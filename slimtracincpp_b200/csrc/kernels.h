@@ -130,6 +130,14 @@ struct BatchFrame {
     const BatchWave *waves;            // host
     uint32_t wave_count;
     const CacheFrame *cache;           // null: no request uses the cache
+    // Waves without cache paths alternate between two lanes (the launching
+    // stream with the first queue set, lane_stream with the second), so the
+    // tail of one wave's persistent launches overlaps the next wave's work;
+    // waves with cache paths stay on the first lane, which owns the cache's
+    // buffers.  Null lane_stream or lane_queues: every wave on one lane.
+    cudaStream_t lane_stream;
+    const WavefrontBuffers *lane_queues;
+    cudaEvent_t lane_fork, lane_join;
 };
 cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
                                 StageTimer *timer);

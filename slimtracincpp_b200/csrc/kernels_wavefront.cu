@@ -1602,7 +1602,7 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
 
 // Batched requests: every wave is a full multi-request frame over its slots.
 template <bool COUNT>
-cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
+cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B0, int block, cudaStream_t stream0,
                       StageTimer *timer) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1610,8 +1610,21 @@ cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block
     const CacheFrame *cache = BF.cache;
     CacheArgs CA = cache_args(cache);
     cudaError_t e;
+    const bool two_lanes = BF.lane_stream && BF.lane_queues;
+    if (two_lanes) {
+        if ((e = cudaEventRecord(BF.lane_fork, stream0)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(BF.lane_stream, BF.lane_fork, 0)) != cudaSuccess) return e;
+    }
+    uint32_t next_lane = 0;
     for (uint32_t wi = 0; wi < BF.wave_count; wi++) {
         const BatchWave &wave = BF.waves[wi];
+        uint32_t lane = 0;
+        if (two_lanes && !(cache && wave.cache_paths)) {
+            lane = next_lane;
+            next_lane ^= 1u;
+        }
+        const WavefrontBuffers &B = lane ? *BF.lane_queues : B0;
+        const cudaStream_t stream = lane ? BF.lane_stream : stream0;
         RoundLaunch L{&BF.shared, &BF.frame, &B, block <= 0 ? 256 : block, sms, stream, timer, BF.frame.counters,
                       B.capacity, wave.max_lights, BF.shared.mesh_count > 0};
         if ((e = cudaMemsetAsync(B.queue_count, 0, 8 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
@@ -1650,6 +1663,10 @@ cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block
             if ((e = trace_round<COUNT, true>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
         }
         if (use_cache && (e = cache_phase<COUNT, true>(L, A, CA, in, cache, wave.max_depth)) != cudaSuccess) return e;
+    }
+    if (two_lanes) {
+        if ((e = cudaEventRecord(BF.lane_join, BF.lane_stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(stream0, BF.lane_join, 0)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }

@@ -493,41 +493,112 @@ SLIM_D bool leaf_round(bool waiting, bool can_step) {
 // pass alone).
 constexpr int kMeshBlock = 128;
 
+// Drain phase of the persistent any-hit kernel.  Once the pair queue is
+// empty, a lane with nothing left to walk takes the deepest pending subtree
+// (the bottom entry of the stack) of a lane of its warp that is still
+// walking, so the last long walks of a launch spread over the warp instead
+// of running one lane each while the rest of the warp waits.  The i-th idle
+// lane (in lane order) takes from the i-th lane with a pending subtree; the
+// giver removes the entry from its stack.  Exact: an any-hit result is the
+// OR over the leaves a walk reaches, whatever the order (config 2: 1.46 ->
+// 1.45 ms; config 4's plain depth-8 frame, whose late rounds are almost all
+// tail: 3.00 -> 2.91 ms).  The closest-hit walks do not share: a piece that
+// does not know the best hit of the part before it in the reference's order
+// could report a triangle the reference culls.
+struct Steal {
+    int from;           // giving lane for a taker, else -1
+    uint32_t subtree;   // stack entry handed over (valid for a taker)
+};
+SLIM_D Steal steal_round(uint32_t act, uint32_t idle_mask, uint32_t donor_mask, bool idle, bool donor,
+                         uint32_t *stack, uint32_t &bottom, uint32_t &top) {
+    const uint32_t below = (1u << lane_id()) - 1u;
+    const uint32_t pairs = min((uint32_t)__popc(idle_mask), (uint32_t)__popc(donor_mask));
+    const uint32_t my_idle_rank = (uint32_t)__popc(idle_mask & below);
+    const bool taker = idle && my_idle_rank < pairs;
+    const bool giver = donor && (uint32_t)__popc(donor_mask & below) < pairs;
+    uint32_t give = 0;
+    if (giver) {
+        give = stack[bottom++];
+        if (bottom == top) bottom = top = 0;
+    }
+    uint32_t m = donor_mask;
+    for (uint32_t j = 0; taker && j < my_idle_rank; j++) m &= m - 1u;
+    const int src = taker ? __ffs(m) - 1 : (int)lane_id();
+    Steal st;
+    st.subtree = __shfl_sync(act, give, src);
+    st.from = taker ? src : -1;
+    return st;
+}
+// Stack push for walks that may give entries away from the bottom: the live
+// entries are [bottom, top); when the top reaches the capacity they move
+// down first.  Returns false on overflow.
+SLIM_D bool push_entry(uint32_t *stack, uint32_t &bottom, uint32_t &top, uint32_t v) {
+    if (top >= (uint32_t)kStackCapacity) {
+        if (bottom == 0) return false;
+        for (uint32_t i = bottom; i < top; i++) stack[i - bottom] = stack[i];
+        top -= bottom;
+        bottom = 0;
+    }
+    stack[top++] = v;
+    return true;
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
     const uint32_t n = *A.pair_count < A.pair_capacity ? *A.pair_count : A.pair_capacity;
     uint32_t stack[kStackCapacity];
     uint32_t err = 0;
     Work w = {};
-    bool busy = false, walking = false;
-    uint32_t tag = 0, left = 0, top = 0, tri_offset = 0;
+    bool busy = false, walking = false, drained = false;
+    uint32_t idx = 0, tag = 0, left = 0, top = 0, bottom = 0, tri_offset = 0;
     const float4 *nodes = nullptr;
     float aux = 0.0f;
     Ray r;
     PendingLeaves pend;
     pend.n = 0;
+    // (shadow ray, instance) pair i from its root's children, or from `subtree`
+    auto start = [&](uint32_t i, uint32_t subtree, bool whole) {
+        const float4 *p = A.pairs + 3 * (size_t)i;
+        float4 p0 = p[0], p1 = p[1], p2 = p[2];
+        tag = __float_as_uint(p1.w);
+        if ((A.masks[tag >> 6] >> (tag & 63u)) & 1ull) return;   // already known occluded
+        idx = i;
+        reset(r, xyz(p0), xyz(p1));
+        aux = p0.w;
+        nodes = S.mesh_nodes + 2 * (size_t)__float_as_uint(p2.x);
+        tri_offset = __float_as_uint(p2.y);
+        left = whole ? __float_as_uint(p2.z) : subtree;
+        top = bottom = 0;
+        pend.n = 0;
+        busy = walking = true;
+    };
     for (;;) {
-        const bool fetch = fetch_round(!busy);
-        if (!busy && fetch) {
-            uint32_t active = __activemask();
-            int leader = __ffs(active) - 1;
-            uint32_t base = 0;
-            if ((int)lane_id() == leader) base = atomicAdd(A.pair_cursor, (uint32_t)__popc(active));
-            base = __shfl_sync(active, base, leader);
-            uint32_t idx = base + (uint32_t)__popc(active & ((1u << lane_id()) - 1u));
-            if (idx >= n) break;
-            const float4 *p = A.pairs + 3 * (size_t)idx;
-            float4 p0 = p[0], p1 = p[1], p2 = p[2];
-            tag = __float_as_uint(p1.w);
-            if ((A.masks[tag >> 6] >> (tag & 63u)) & 1ull) continue;   // already known occluded
-            reset(r, xyz(p0), xyz(p1));
-            aux = p0.w;
-            nodes = S.mesh_nodes + 2 * (size_t)__float_as_uint(p2.x);
-            tri_offset = __float_as_uint(p2.y);
-            left = __float_as_uint(p2.z);
-            top = 0;
-            pend.n = 0;
-            busy = walking = true;
+        if (!drained) {
+            const bool fetch = fetch_round(!busy);
+            if (!busy && fetch) {
+                uint32_t active = __activemask();
+                int leader = __ffs(active) - 1;
+                uint32_t base = 0;
+                if ((int)lane_id() == leader) base = atomicAdd(A.pair_cursor, (uint32_t)__popc(active));
+                base = __shfl_sync(active, base, leader);
+                const uint32_t i = base + (uint32_t)__popc(active & ((1u << lane_id()) - 1u));
+                if (i >= n) drained = true;
+                else start(i, 0, true);
+            }
+        }
+        {
+            const uint32_t act = __activemask();
+            if (__ballot_sync(act, drained)) {
+                const uint32_t idle = __ballot_sync(act, drained && !busy);
+                if (idle == act) break;
+                const bool donor = walking && top > bottom;
+                const uint32_t donors = __ballot_sync(act, donor);
+                if (idle && donors) {
+                    const Steal st = steal_round(act, idle, donors, drained && !busy, donor, stack, bottom, top);
+                    const uint32_t from_idx = __shfl_sync(act, idx, st.from >= 0 ? st.from : (int)lane_id());
+                    if (st.from >= 0) start(from_idx, st.subtree, false);
+                }
+            }
         }
 #pragma unroll
         for (uint32_t sub = 0; sub < kStepsPerTurn; sub++) if (walking && pend.can_step()) {
@@ -546,14 +617,14 @@ __global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFr
             bool go_left = hl && !lcount, go_right = hr && !rcount;
             if (go_left) {
                 if (go_right) {
-                    if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; walking = false; }
-                    else stack[top++] = rc;
+                    if (!push_entry(stack, bottom, top, rc)) { err |= kErrStack; walking = false; }
                 }
                 left = lc;
             } else if (go_right) {
                 left = rc;
-            } else if (top == 0) {
+            } else if (top == bottom) {
                 walking = false;
+                top = bottom = 0;
             } else {
                 left = stack[--top];
             }
@@ -567,6 +638,7 @@ __global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFr
             if (hit) {
                 atomicOr(A.masks + (tag >> 6), 1ull << (tag & 63u));
                 walking = false;
+                top = bottom = 0;
                 pend.n = 0;
             }
         }

@@ -470,6 +470,11 @@ int upload_meshes(Context &c, const SlimSceneData *s) {
         if (!m.triangles || !m.triangle_count) return set_error(SLIM_ERR_ARGUMENT, "mesh has no triangles");
         int rc = check_bvh(m.bvh.nodes, m.bvh.node_count, m.triangle_count, 0, "mesh BVH malformed");
         if (rc) return rc;
+        if (m.triangle_count >= (1u << kLeafCountShift))
+            return set_error(SLIM_ERR_LIMIT, "mesh has 2^26 triangles or more");
+        for (uint32_t k = 1; k < m.bvh.node_count; k++)   // a root leaf is tested without being packed
+            if (m.bvh.nodes[k].leaf_count >= (1u << (32 - kLeafCountShift)))
+                return set_error(SLIM_ERR_LIMIT, "mesh BVH leaf below the root holds 64 triangles or more");
         uint32_t d = bvh_depth(m.bvh.nodes, m.bvh.node_count);
         if (d + 2 > (uint32_t)kStackCapacity) return set_error(SLIM_ERR_LIMIT, "mesh BVH deeper than the traversal stack (62 levels)");
         if (d > c.max_mesh_height) c.max_mesh_height = d;

@@ -18,7 +18,12 @@
 
 namespace slim {
 
-constexpr int kStackCapacity = 64;        // per-ray traversal stack entries (scene and mesh)
+constexpr int kStackCapacity = 64;
+// Mesh-BVH leaves waiting in the persistent mesh kernels are packed as
+// first triangle | count << kLeafCountShift: meshes hold fewer than 2^26
+// triangles and leaves below the root fewer than 64 (checked on upload; the
+// reference's builder makes leaves of at most two).
+constexpr uint32_t kLeafCountShift = 26;        // per-ray traversal stack entries (scene and mesh)
 constexpr int kMaxLights = 64;            // lights a shadow mask can track
 constexpr uint32_t kErrStack = 1u;        // device error bits
 constexpr uint32_t kErrIndex = 2u;

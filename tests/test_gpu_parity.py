@@ -327,3 +327,21 @@ def test_pageable_canvas_through_pinned_staging():
     torch.cuda.synchronize()
     assert np.array_equal(pix.view(np.uint32), d_pix.cpu().numpy().view(np.uint32))
     assert np.array_equal(dep.view(np.uint32), d_dep.cpu().numpy().view(np.uint32))
+
+
+def test_mesh_leaf_too_large_for_the_packed_record_is_refused():
+    """The persistent mesh kernels pack a waiting leaf into one word (first
+    triangle, count below 64); a mesh whose BVH has a larger leaf below the
+    root is refused on upload with SLIM_ERR_LIMIT instead of being traced
+    wrong.  A root leaf of any size is fine (tested without packing)."""
+    from slimtracincpp_b200.scene import MeshAsset, Scene, geometry
+    pos, idx, nrm = scenes.icosphere(2)
+    mesh = MeshAsset.build(pos, idx, nrm, idx)
+    assert mesh.triangle_count >= 64
+    mesh.nodes["leaf_count"][1] = 64
+    mesh.nodes["first_index"][1] = 0
+    g = geometry(L.GEOMETRY_MESH, 0)
+    scene = Scene(np.array([g]), np.array([L.default_material()]), meshes=[mesh])
+    with pytest.raises(native.SlimError) as err:
+        RayTracingRenderer(scene, max_depth=1)
+    assert err.value.code == 4 and "64 triangles" in str(err.value)

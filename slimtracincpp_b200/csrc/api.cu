@@ -158,7 +158,8 @@ struct Context {
     PinnedBuffer stage_pixels, stage_depths;     // pageable canvases: the frame lands here first
     HostCopyPool copy_pool;
     cudaEvent_t refit_done = nullptr;            // the last scene BVH refit, on the caller's stream
-    std::vector<cudaEvent_t> band_events;        // one per band, the last marks the downloads' end
+    std::vector<cudaEvent_t> band_events;        // three per band (depths, first round, copies), then one
+                                                 // per lane marking the downloads' end
     SlimSceneCounts counts{};
     std::vector<SlimGeometry> geometries;
     std::vector<SlimMaterial> materials;
@@ -948,7 +949,7 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     for (int l = 0; banded_download && l < kBandLanes; l++)
         if (!c.copy_streams[l])
             SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_streams[l], cudaStreamNonBlocking), "copy stream");
-    while (c.band_events.size() < 2 * bands + kBandLanes) {
+    while (c.band_events.size() < 3 * bands + kBandLanes) {
         cudaEvent_t e;
         SLIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
         c.band_events.push_back(e);
@@ -991,8 +992,9 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         if (early) {
             FrameDownload dl{};
             dl.copy_stream = c.copy_streams[lane];
-            dl.round_done = c.band_events[2 * b];
-            dl.copied = c.band_events[2 * b + 1];
+            dl.depths_done = c.band_events[3 * b];
+            dl.round_done = c.band_events[3 * b + 1];
+            dl.copied = c.band_events[3 * b + 2];
             dl.host_pixels = host_pixels + p0;
             dl.host_depths = host_depths + d0;
             dl.dev_pixels = d_pixels + p0;
@@ -1024,8 +1026,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     }
     if (banded_download) {
         for (int l = 0; l < kBandLanes; l++) {
-            SLIM_CUDA(cudaEventRecord(c.band_events[2 * bands + l], c.copy_streams[l]), "downloads done");
-            SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[2 * bands + l], 0), "downloads done");
+            SLIM_CUDA(cudaEventRecord(c.band_events[3 * bands + l], c.copy_streams[l]), "downloads done");
+            SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[3 * bands + l], 0), "downloads done");
         }
     } else if (download) {
         SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, stream),

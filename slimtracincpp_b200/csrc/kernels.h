@@ -98,7 +98,7 @@ struct CacheFrame {
 // address space), once the copy has landed.
 struct FrameDownload {
     cudaStream_t copy_stream;
-    cudaEvent_t round_done, copied;       // recorded by the launcher
+    cudaEvent_t depths_done, round_done, copied;  // recorded by the launcher
     void *host_pixels, *host_depths;      // destinations of the copies
     const void *dev_pixels, *dev_depths;  // sources of the copies
     size_t pixel_bytes, depth_bytes;

@@ -110,6 +110,7 @@ struct QueueArgs {
     uint32_t samples;
     uint32_t depth;               // 1-based bounce of this round
     uint32_t light_begin, light_end;
+    uint32_t early_depth;         // non-zero: shadow_gen writes every path's canvas depth, shade only colours
     unsigned long long *counters; // this stage's counter slots, or null
     // radiance cache
     float4 *sink;                 // non-null: finished paths write their linear colour here
@@ -190,10 +191,12 @@ template <bool BATCH> SLIM_D float cone_scaling(const DevFrame &F, uint32_t pid)
     uint32_t p = pix_of<BATCH>(pid);
     return F.cones_per_pixel ? pixel_scaling(F.projection, (int)(p % F.width), (int)(p / F.width)) : 0.0f;
 }
-template <bool BATCH> SLIM_D void write_pixel(const DevFrame &F, uint32_t pid, float3 color, float depth) {
+template <bool BATCH>
+SLIM_D void write_pixel(const DevFrame &F, uint32_t pid, float3 color, float depth, bool with_depth = true) {
     uint32_t p = pix_of<BATCH>(pid);
     float3 c = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
-    set_pixel(F, (int)(p % F.width), (int)(p / F.width), c, depth);
+    if (with_depth) set_pixel(F, (int)(p % F.width), (int)(p / F.width), c, depth);
+    else set_pixel_color(F, (int)(p % F.width), (int)(p / F.width), c);
 }
 
 SLIM_D uint32_t queue_size(const QueueArgs &A) { return A.count_in ? *A.count_in : A.samples; }
@@ -229,6 +232,9 @@ template <bool BATCH> SLIM_D bool at_cache_vertex(const DevFrame &F, const Queue
 }
 
 // ---- shadow_gen: one shadow ray per facing, shadowing light -------------
+// In a single frame's first round it can also write the canvas depths (the
+// shaded hit's depth, infinity where shade leaves none), which are final
+// once the primary hits are: they download while the shadows are traced.
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
@@ -261,6 +267,10 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, Qu
                     prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
                     shaded = true;
                 }
+            }
+            if (!BATCH && A.early_depth && A.light_begin == 0) {
+                uint32_t p = pix_of<BATCH>(pid);
+                set_depth(F, (int)(p % F.width), (int)(p / F.width), shaded ? depth_at(F.projection, hit.position) : INFINITY);
             }
         }
         for (uint32_t li = A.light_begin; li < A.light_end; li++) {
@@ -1229,7 +1239,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, Queu
                 } else if (A.sink) {
                     A.sink[path] = make_float4(color.x, color.y, color.z, 0.0f);
                 } else {
-                    write_pixel<BATCH>(F, pid, color, depth);
+                    write_pixel<BATCH>(F, pid, color, depth, BATCH || !A.early_depth);
                 }
             }
         }
@@ -1361,6 +1371,7 @@ struct RoundLaunch {
     bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
     cudaEvent_t pixel_wait = nullptr;  // kernels that write pixels wait for it (a download in flight)
+    const FrameDownload *depth_download = nullptr;  // first round: the depths download after shadow_gen
     unsigned long long *stage(int st) const { return counters ? counters + kCountersPerStage * st : nullptr; }
     uint32_t grid(const void *kernel, uint32_t work) const { return grid_for(kernel, work, block); }
     // the persistent mesh kernels run 128-thread blocks (kMeshBlock)
@@ -1466,6 +1477,14 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         k_shadow_gen<COUNT, BATCH><<<L.grid((const void *)k_shadow_gen<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
         count_launch();
         if (timer) timer->end(STAGE_SHADOW_GEN, stream);
+        if (l0 == 0 && A.early_depth && L.depth_download) {
+            const FrameDownload *dl = L.depth_download;
+            if ((r = cudaEventRecord(dl->depths_done, stream)) != cudaSuccess) return r;
+            if ((r = cudaStreamWaitEvent(dl->copy_stream, dl->depths_done, 0)) != cudaSuccess) return r;
+            if ((r = cudaMemcpyAsync(dl->host_depths, dl->dev_depths, dl->depth_bytes, cudaMemcpyDeviceToHost,
+                                     dl->copy_stream)) != cudaSuccess)
+                return r;
+        }
         r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
         if (r != cudaSuccess) return r;
         A.counters = L.stage(STAGE_SHADOW);
@@ -1658,8 +1677,15 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
             if ((e = tail_round<COUNT, false>(L, A, in, depth)) != cudaSuccess) return e;
             break;
         }
+        // the depths are final after the first round's shadow_gen (which
+        // needs a light to run): they download while the shadows are traced
+        const bool early_depth = depth == 1 && dl && !use_cache && L.lights > 0;
+        A.early_depth = early_depth;
+        L.depth_download = early_depth ? dl : nullptr;
         if ((e = trace_round<COUNT, false>(L, A, CA, in, depth, depth == 1, use_cache && depth == last)) != cudaSuccess)
             return e;
+        A.early_depth = 0;
+        L.depth_download = nullptr;
         if (depth == 1 && dl && !use_cache) {
             // every path that ended at its first hit has written its pixel:
             // the rows go to the host now; later pixels go there directly
@@ -1668,8 +1694,8 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
             if ((e = cudaMemcpyAsync(dl->host_pixels, dl->dev_pixels, dl->pixel_bytes, cudaMemcpyDeviceToHost,
                                      dl->copy_stream)) != cudaSuccess)
                 return e;
-            if ((e = cudaMemcpyAsync(dl->host_depths, dl->dev_depths, dl->depth_bytes, cudaMemcpyDeviceToHost,
-                                     dl->copy_stream)) != cudaSuccess)
+            if (!early_depth && (e = cudaMemcpyAsync(dl->host_depths, dl->dev_depths, dl->depth_bytes,
+                                                     cudaMemcpyDeviceToHost, dl->copy_stream)) != cudaSuccess)
                 return e;
             if ((e = cudaEventRecord(dl->copied, dl->copy_stream)) != cudaSuccess) return e;
             late.pixels = dl->mapped_pixels;

@@ -972,14 +972,21 @@ SLIM_D float depth_at(const SlimCameraRayProjection &p, float3 pos) {           
     return m[2] * v.x + m[5] * v.y + m[8] * v.z;
 }
 
-// Canvas::setPixel(x, y, color, -1, depth) (draw/canvas.h:128-165).
-SLIM_D void set_pixel(const DevFrame &F, int x, int y, float3 c, float depth) {
-    c = f3(clamp01(c.x), clamp01(c.y), clamp01(c.z));
-    c = c * (c * 1.0f);
-    uint32_t offset = F.antialias == SLIM_AA_SSAA
+// Canvas::setPixel(x, y, color, -1, depth) (draw/canvas.h:128-165), in two
+// halves so a frame can write its depths before its colours are final.
+// Canvas entry of a sample: SSAA keeps a pixel's four samples together.
+SLIM_D uint32_t canvas_offset(const DevFrame &F, int x, int y) {
+    return F.antialias == SLIM_AA_SSAA
         ? ((F.stride * (uint32_t)(y >> 1) + (uint32_t)(x >> 1)) * 4 + 2 * (uint32_t)(y & 1) + (uint32_t)(x & 1))
         : (F.stride * (uint32_t)y + (uint32_t)x);
-    F.pixels[offset] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+SLIM_D void set_pixel_color(const DevFrame &F, int x, int y, float3 c) {
+    c = f3(clamp01(c.x), clamp01(c.y), clamp01(c.z));
+    c = c * (c * 1.0f);
+    F.pixels[canvas_offset(F, x, y)] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+SLIM_D void set_depth(const DevFrame &F, int x, int y, float depth) {
+    uint32_t offset = canvas_offset(F, x, y);
     if (F.antialias == SLIM_AA_MSAA) {
         F.depths[offset * 4] = depth;
         F.depths[offset * 4 + 1] = 0;
@@ -988,6 +995,10 @@ SLIM_D void set_pixel(const DevFrame &F, int x, int y, float3 c, float depth) {
     } else {
         F.depths[offset] = depth;
     }
+}
+SLIM_D void set_pixel(const DevFrame &F, int x, int y, float3 c, float depth) {
+    set_pixel_color(F, x, y, c);
+    set_depth(F, x, y, depth);
 }
 
 }  // namespace dev

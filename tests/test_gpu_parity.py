@@ -15,6 +15,7 @@ import pytest
 from slimtracincpp_b200 import layout as L
 from slimtracincpp_b200 import native, scenes
 from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport
+from slimtracincpp_b200.scene import Scene
 from oracle import bindings as O
 
 pytestmark = pytest.mark.gpu
@@ -237,9 +238,18 @@ def test_pick_selects_a_light_in_front_of_the_geometry():
     assert int(far["light"]) == -1
 
 
+def _without_lights(w):
+    """The workload with every light removed (the scene is rebuilt)."""
+    sc = w.scene
+    w.scene = Scene(sc.geometries, sc.materials, np.zeros(0, L.LIGHT), meshes=sc.meshes, textures=sc.textures)
+    return w
+
+
 BANDED_SCENES = {
     "mesh_depth2": lambda: scenes.small_mesh_scene(0, 120, 70),
     "implicit_depth6": lambda: scenes.feature_scene(4, 120, 70, max_depth=6),   # late bounces in the fused tail
+    # no shadow rays: the depths download with the pixels, not before them
+    "mesh_no_lights": lambda: _without_lights(scenes.small_mesh_scene(2, 120, 70)),
 }
 
 
@@ -249,10 +259,11 @@ BANDED_SCENES = {
 def test_banded_download_into_a_pinned_canvas(engine, antialias, scene):
     """slimRenderOnGPU renders the frame in row bands, two in flight on two
     streams.  Into pinned host memory each band's rows download once its
-    first round is done, and the pixels of later bounces are written into the
-    host canvas directly: the canvas must equal the one-band frame bit for
-    bit, for any band count (70 rows: the last band also holds the rows past
-    the last 4-row tile band)."""
+    first round is done (its depths, when the scene has lights, once the
+    primary hits are shaded for shadow rays), and the pixels of later bounces
+    are written into the host canvas directly: the canvas must equal the
+    one-band frame bit for bit, for any band count (70 rows: the last band
+    also holds the rows past the last 4-row tile band)."""
     from slimtracincpp_b200.renderer import make_canvas
     w = BANDED_SCENES[scene]()
     r = renderer_for(w)

@@ -158,7 +158,7 @@ struct Context {
     PinnedBuffer stage_pixels, stage_depths;     // pageable canvases: the frame lands here first
     HostCopyPool copy_pool;
     cudaEvent_t refit_done = nullptr;            // the last scene BVH refit, on the caller's stream
-    std::vector<cudaEvent_t> band_events;        // three per band (depths, first round, copies), then one
+    std::vector<cudaEvent_t> band_events;        // per band: depths, copies and one per pixel chunk; then one
                                                  // per lane marking the downloads' end
     SlimSceneCounts counts{};
     std::vector<SlimGeometry> geometries;
@@ -949,7 +949,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     for (int l = 0; banded_download && l < kBandLanes; l++)
         if (!c.copy_streams[l])
             SLIM_CUDA(cudaStreamCreateWithFlags(&c.copy_streams[l], cudaStreamNonBlocking), "copy stream");
-    while (c.band_events.size() < 3 * bands + kBandLanes) {
+    constexpr uint32_t kEventsPerBand = 2 + kPixelChunks;
+    while (c.band_events.size() < kEventsPerBand * bands + kBandLanes) {
         cudaEvent_t e;
         SLIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
         c.band_events.push_back(e);
@@ -992,15 +993,15 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         if (early) {
             FrameDownload dl{};
             dl.copy_stream = c.copy_streams[lane];
-            dl.depths_done = c.band_events[3 * b];
-            dl.round_done = c.band_events[3 * b + 1];
-            dl.copied = c.band_events[3 * b + 2];
+            dl.depths_done = c.band_events[kEventsPerBand * b];
+            dl.copied = c.band_events[kEventsPerBand * b + 1];
+            for (uint32_t k = 0; k < kPixelChunks; k++) dl.pixels_done[k] = c.band_events[kEventsPerBand * b + 2 + k];
             dl.host_pixels = host_pixels + p0;
             dl.host_depths = host_depths + d0;
             dl.dev_pixels = d_pixels + p0;
             dl.dev_depths = d_depths + d0;
-            dl.pixel_bytes = pn * sizeof(float4);
             dl.depth_bytes = dn * sizeof(float);
+            dl.pixel_row_bytes = pix_per_row * sizeof(float4);
             dl.mapped_pixels = mapped_pixels;
             dl.mapped_depths = mapped_depths;
             if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane, &dl)))
@@ -1026,8 +1027,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     }
     if (banded_download) {
         for (int l = 0; l < kBandLanes; l++) {
-            SLIM_CUDA(cudaEventRecord(c.band_events[3 * bands + l], c.copy_streams[l]), "downloads done");
-            SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[3 * bands + l], 0), "downloads done");
+            SLIM_CUDA(cudaEventRecord(c.band_events[kEventsPerBand * bands + l], c.copy_streams[l]), "downloads done");
+            SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_events[kEventsPerBand * bands + l], 0), "downloads done");
         }
     } else if (download) {
         SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost, stream),

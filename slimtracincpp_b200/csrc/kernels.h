@@ -96,12 +96,15 @@ struct CacheFrame {
 // the host then, on copy_stream; the later rounds write the pixels they
 // finish straight into the host canvas (pinned and mapped into the device's
 // address space), once the copy has landed.
+constexpr uint32_t kPixelChunks = 2;     // first-round shade launches, each followed by its rows' copy
 struct FrameDownload {
     cudaStream_t copy_stream;
-    cudaEvent_t depths_done, round_done, copied;  // recorded by the launcher
+    cudaEvent_t depths_done, copied;      // recorded by the launcher
+    cudaEvent_t pixels_done[kPixelChunks];
     void *host_pixels, *host_depths;      // destinations of the copies
     const void *dev_pixels, *dev_depths;  // sources of the copies
-    size_t pixel_bytes, depth_bytes;
+    size_t depth_bytes;
+    size_t pixel_row_bytes;               // canvas pixel bytes per sample row
     float4 *mapped_pixels;                // the whole host canvas, as the device sees it
     float *mapped_depths;
 };

@@ -111,6 +111,7 @@ struct QueueArgs {
     uint32_t depth;               // 1-based bounce of this round
     uint32_t light_begin, light_end;
     uint32_t early_depth;         // non-zero: shadow_gen writes every path's canvas depth, shade only colours
+    uint32_t slot_begin, slot_end;  // shade: the slots [begin, end) of the queue (end 0: all)
     unsigned long long *counters; // this stage's counter slots, or null
     // radiance cache
     float4 *sink;                 // non-null: finished paths write their linear colour here
@@ -1164,10 +1165,12 @@ SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], floa
 template <bool COUNT, bool BATCH>
 __global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
+    if (A.slot_end && A.slot_end < n) n = A.slot_end;
+    const uint32_t first = A.slot_begin;
     Work w = {};
     uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t rounds = (n + stride - 1) / stride;
-    for (uint32_t r = 0, slot = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
+    uint32_t rounds = n > first ? (n - first + stride - 1) / stride : 0;
+    for (uint32_t r = 0, slot = first + blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, slot += stride) {
         bool live = slot < n;
         bool bounce = false, query = false;
         uint32_t path = 0, pid = 0;
@@ -1372,6 +1375,7 @@ struct RoundLaunch {
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
     cudaEvent_t pixel_wait = nullptr;  // kernels that write pixels wait for it (a download in flight)
     const FrameDownload *depth_download = nullptr;  // first round: the depths download after shadow_gen
+    const FrameDownload *pixel_download = nullptr;  // first round: each shade chunk's rows download after it
     unsigned long long *stage(int st) const { return counters ? counters + kCountersPerStage * st : nullptr; }
     uint32_t grid(const void *kernel, uint32_t work) const { return grid_for(kernel, work, block); }
     // the persistent mesh kernels run 128-thread blocks (kMeshBlock)
@@ -1503,8 +1507,31 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
     if (L.pixel_wait && (r = cudaStreamWaitEvent(stream, L.pixel_wait, 0)) != cudaSuccess) return r;
     A.counters = L.stage(STAGE_SHADE);
     if (timer) timer->begin(STAGE_SHADE, stream);
-    k_shade<COUNT, BATCH><<<L.grid((const void *)k_shade<COUNT, BATCH>, L.bound), L.block, 0, stream>>>(S, F, A);
-    count_launch();
+    // A downloaded frame's first round shades its primary paths (slot =
+    // sample, in row order) in chunks of whole 4-row tiles; each chunk's rows
+    // start crossing PCIe while the next chunk shades.
+    const FrameDownload *dl = L.pixel_download;
+    const uint32_t chunks = dl ? kPixelChunks : 1u, tiles = (F.rows + 3) / 4;
+    for (uint32_t c = 0; c < chunks; c++) {
+        const uint32_t r0 = 4 * (tiles * c / chunks), r1 = c + 1 == chunks ? F.rows : 4 * (tiles * (c + 1) / chunks);
+        if (dl) {
+            A.slot_begin = r0 * F.width;
+            A.slot_end = r1 * F.width;
+            if (r1 == r0) continue;
+        }
+        k_shade<COUNT, BATCH><<<L.grid((const void *)k_shade<COUNT, BATCH>, dl ? A.slot_end - A.slot_begin : L.bound),
+                                L.block, 0, stream>>>(S, F, A);
+        count_launch();
+        if (dl) {
+            if ((r = cudaEventRecord(dl->pixels_done[c], stream)) != cudaSuccess) return r;
+            if ((r = cudaStreamWaitEvent(dl->copy_stream, dl->pixels_done[c], 0)) != cudaSuccess) return r;
+            if ((r = cudaMemcpyAsync((char *)dl->host_pixels + r0 * dl->pixel_row_bytes,
+                                     (const char *)dl->dev_pixels + r0 * dl->pixel_row_bytes,
+                                     (r1 - r0) * dl->pixel_row_bytes, cudaMemcpyDeviceToHost, dl->copy_stream)) != cudaSuccess)
+                return r;
+        }
+    }
+    A.slot_begin = A.slot_end = 0;
     if (timer) timer->end(STAGE_SHADE, stream);
     in = out;
     return cudaGetLastError();
@@ -1682,18 +1709,16 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
         const bool early_depth = depth == 1 && dl && !use_cache && L.lights > 0;
         A.early_depth = early_depth;
         L.depth_download = early_depth ? dl : nullptr;
+        // every path that ends at its first hit writes its pixel in this
+        // round's shading: the rows go to the host chunk by chunk
+        L.pixel_download = depth == 1 && !use_cache ? dl : nullptr;
         if ((e = trace_round<COUNT, false>(L, A, CA, in, depth, depth == 1, use_cache && depth == last)) != cudaSuccess)
             return e;
         A.early_depth = 0;
-        L.depth_download = nullptr;
+        L.depth_download = L.pixel_download = nullptr;
         if (depth == 1 && dl && !use_cache) {
-            // every path that ended at its first hit has written its pixel:
-            // the rows go to the host now; later pixels go there directly
-            if ((e = cudaEventRecord(dl->round_done, stream)) != cudaSuccess) return e;
-            if ((e = cudaStreamWaitEvent(dl->copy_stream, dl->round_done, 0)) != cudaSuccess) return e;
-            if ((e = cudaMemcpyAsync(dl->host_pixels, dl->dev_pixels, dl->pixel_bytes, cudaMemcpyDeviceToHost,
-                                     dl->copy_stream)) != cudaSuccess)
-                return e;
+            // the copy stream is past the round's last shade chunk: later
+            // pixels go to the host canvas directly once the copies landed
             if (!early_depth && (e = cudaMemcpyAsync(dl->host_depths, dl->dev_depths, dl->depth_bytes,
                                                      cudaMemcpyDeviceToHost, dl->copy_stream)) != cudaSuccess)
                 return e;

@@ -507,6 +507,14 @@ int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_
                     uint32_t flags, SlimTexture *texture, SlimTextureMip *mips,
                     SlimTexelQuad *texel_quads, uint32_t *mip_count, uint32_t *texel_quad_count);
 
+/* The same bake on the GPU (the converter bmp2texture.cpp:24-335 runs on the
+ * host in the reference): same arguments, same two-call protocol, the same
+ * bytes as slimBakeTexture.  Host buffers in and out; the image crosses to
+ * the device, the texel quads come back before the call returns. */
+int slimBakeTextureOnGPU(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels,
+                         uint32_t flags, SlimTexture *texture, SlimTextureMip *mips,
+                         SlimTexelQuad *texel_quads, uint32_t *mip_count, uint32_t *texel_quad_count);
+
 #ifdef __cplusplus
 }
 #endif

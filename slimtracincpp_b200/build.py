@@ -25,7 +25,8 @@ OUT_DIR = PKG / "_native"
 LIB = OUT_DIR / "libslimtracer_b200.so"
 BUILD_DIR = ROOT / "_build" / "slimtracer"
 
-CUDA_SOURCES = ["api.cu", "kernels_fused.cu", "kernels_wavefront.cu", "kernels_refit.cu", "kernels_nrc.cu"]
+CUDA_SOURCES = ["api.cu", "kernels_fused.cu", "kernels_wavefront.cu", "kernels_refit.cu", "kernels_nrc.cu",
+                "kernels_bake.cu"]
 HOST_SOURCES = ["host_assets.cpp", "texture_baker.cpp"]
 HEADERS = ["device_scene.h", "host_common.h", "kernels.h", "tracer_core.cuh", "nrc.h", "umma.cuh", "launch_count.h"]
 

@@ -1319,6 +1319,17 @@ int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_
                     uint32_t *texel_quad_count) {
     return slim::bake_texture(bgr, width, height, channels, flags, texture, mips, texel_quads, mip_count, texel_quad_count);
 }
+int slimBakeTextureOnGPU(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
+                         SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *texel_quads, uint32_t *mip_count,
+                         uint32_t *texel_quad_count) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (texel_quads && mips) {   // the sizing call needs no device
+        int rc = ensure_device(g_ctx);
+        if (rc) return rc;
+    }
+    return slim::bake_texture_gpu(bgr, width, height, channels, flags, texture, mips, texel_quads, mip_count,
+                                  texel_quad_count, g_ctx.stream);
+}
 
 }  // extern "C"
 

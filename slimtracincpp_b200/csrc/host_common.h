@@ -27,5 +27,6 @@ int write_texture(const char *path, const SlimTexture *t);
 int bake_texture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
                  SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *quads, uint32_t *mip_count,
                  uint32_t *quad_count);
+float bake_component(uint8_t c, bool linear);
 
 }  // namespace slim

@@ -150,4 +150,10 @@ cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B,
 cudaError_t launch_refit_scene_bvh(const DevScene &S, float4 *scene_nodes, const uint32_t *parent_order,
                                    uint32_t node_count, cudaStream_t stream, StageTimer *timer);
 
+// bmp2texture's texel-quad baker on the device (kernels_bake.cu): the
+// arguments and results of slimBakeTexture, on `stream`, synchronous.
+int bake_texture_gpu(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
+                     SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *quads, uint32_t *mip_count,
+                     uint32_t *quad_count, cudaStream_t stream);
+
 }  // namespace slim

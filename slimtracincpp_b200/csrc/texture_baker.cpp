@@ -173,6 +173,13 @@ inline uint8_t to_byte(float v) { return (uint8_t)(v * 255.0f); }
 
 }  // namespace
 
+// The colour value component_pixel gives an 8-bit component: the device
+// baker's lookup table.
+float bake_component(uint8_t c, bool linear) {
+    const uint8_t bgr[3] = {c, c, c};
+    return component_pixel(bgr, 3, linear).r;
+}
+
 int bake_texture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
                  SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *quads, uint32_t *mip_count,
                  uint32_t *quad_count) {

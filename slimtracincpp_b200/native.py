@@ -25,6 +25,7 @@ EXPORTS = [
     "slimGetRenderOptions", "slimRenderToDevice", "slimTracePrimary", "slimGetWorkCounters", "slimRefitSceneBVH",
     "slimProjectionReset", "slimBuildSceneBVH", "slimBuildMesh", "slimReadMeshHeader", "slimReadMesh",
     "slimWriteMesh", "slimReadTextureHeader", "slimReadTexture", "slimWriteTexture", "slimBakeTexture",
+    "slimBakeTextureOnGPU",
     "slimGetStageStats", "slimResetStageStats", "slimRenderToDeviceNoAlloc",
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
@@ -74,6 +75,7 @@ def lib():
     h.slimReadTexture.argtypes = [C.c_char_p, P, P, P]
     h.slimWriteTexture.argtypes = [C.c_char_p, P]
     h.slimBakeTexture.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
+    h.slimBakeTextureOnGPU.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
     h.slimGetStageStats.argtypes = [P, C.c_int, P]
     h.slimResetStageStats.argtypes = []
     for name in ["slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheGetStats"]:

@@ -145,18 +145,19 @@ class TextureAsset:
         return self.quads[off:off + (w + 1) * (h + 1)].reshape(h + 1, w + 1)
 
     @classmethod
-    def bake(cls, bgr, flags):
-        """bmp2texture's baker (bmp2texture.cpp:24-335) on 8-bit BGR(A) rows."""
+    def bake(cls, bgr, flags, on_gpu=False):
+        """bmp2texture's baker (bmp2texture.cpp:24-335) on 8-bit BGR(A) rows,
+        on the host or (on_gpu) on the device: the same bytes."""
         img = np.ascontiguousarray(bgr, dtype=np.uint8)
         h, w, ch = img.shape
         mip_count = np.zeros(1, np.uint32)
         quad_count = np.zeros(1, np.uint32)
         header = np.zeros((), L.TEXTURE)
-        check(lib().slimBakeTexture(ptr(img), w, h, ch, flags, ptr(header), 0, 0, ptr(mip_count), ptr(quad_count)))
+        baker = lib().slimBakeTextureOnGPU if on_gpu else lib().slimBakeTexture
+        check(baker(ptr(img), w, h, ch, flags, ptr(header), 0, 0, ptr(mip_count), ptr(quad_count)))
         mips = np.zeros(int(mip_count[0]), L.TEXTURE_MIP)
         quads = np.zeros(int(quad_count[0]), L.TEXEL_QUAD)
-        check(lib().slimBakeTexture(ptr(img), w, h, ch, flags, ptr(header), ptr(mips), ptr(quads), ptr(mip_count),
-                                    ptr(quad_count)))
+        check(baker(ptr(img), w, h, ch, flags, ptr(header), ptr(mips), ptr(quads), ptr(mip_count), ptr(quad_count)))
         return cls(header, [(m["width"], m["height"]) for m in mips], quads)
 
     def save(self, path):

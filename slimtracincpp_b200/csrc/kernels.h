@@ -96,7 +96,7 @@ struct CacheFrame {
 // the host then, on copy_stream; the later rounds write the pixels they
 // finish straight into the host canvas (pinned and mapped into the device's
 // address space), once the copy has landed.
-constexpr uint32_t kPixelChunks = 2;     // first-round shade launches, each followed by its rows' copy
+constexpr uint32_t kPixelChunks = 3;     // first-round shade launches, each followed by its rows' copy
 struct FrameDownload {
     cudaStream_t copy_stream;
     cudaEvent_t depths_done, copied;      // recorded by the launcher

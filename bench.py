@@ -58,6 +58,8 @@ def parse():
                    help="row bands of every wavefront frame (0: the library default; 1: whole frames, as for ncu "
                         "captures of whole-frame launches)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    p.add_argument("--train-samples", type=int, default=65536,
+                   help="radiance cache (config4): training paths per frame, each traced to full depth")
     return p.parse_args()
 
 
@@ -362,7 +364,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     plain_stages = {s["name"]: s["total_ms"] / steps for s in native.stage_stats() if s["launches"]}
 
     # radiance-cache frames (online training continues through warm-up and timing)
-    cache = RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=args.seed)
+    cache = RadianceCache.configure(cache_depth=2, train_samples=args.train_samples, batch=16384, seed=args.seed)
     native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True, radiance_cache=L.CACHE_ON)
     outs = buffers(steps)
     # the cache learns online: its first frames are its warm-up (at least
@@ -450,7 +452,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
             "ms_per_step": cache_total / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded config2 scene, depth 8)",
             "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 8, "cache_depth": 2,
-                       "train_samples_per_frame": 65536, "batch": 16384, "learning_rate": 1e-2,
+                       "train_samples_per_frame": args.train_samples, "batch": 16384, "learning_rate": 1e-2,
                        "cache_warmup_frames": cache_warmup,
                        "engine": "wavefront", "parallelism": f"replicas x{world}",
                        "l2": "flushed between steps (512 MiB write)", "rays_per_frame": cache_rays},

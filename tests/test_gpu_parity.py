@@ -250,6 +250,9 @@ BANDED_SCENES = {
     "implicit_depth6": lambda: scenes.feature_scene(4, 120, 70, max_depth=6),   # late bounces in the fused tail
     # no shadow rays: the depths download with the pixels, not before them
     "mesh_no_lights": lambda: _without_lights(scenes.small_mesh_scene(2, 120, 70)),
+    # fewer tile rows than first-round shade chunks: empty chunks are skipped
+    "mesh_4_rows": lambda: scenes.small_mesh_scene(3, 24, 4),
+    "implicit_6_rows": lambda: scenes.feature_scene(5, 24, 6, max_depth=3),
 }
 
 

@@ -220,80 +220,143 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(workload, seconds, threads=None):
-    """The reference's own CPU renderer (oracle/_ref) on the host cores, on
-    a bounded sample of the same frame: horizontal bands spread over the
-    image until `seconds` of wall time are spent.  Ray counts of the sample
-    come from the oracle's counters for the same rows."""
+def frame_rays(workload):
+    """Rays of one frame in the reference's order (primary + shadow +
+    bounce), counted by the oracle on every host core."""
+    from oracle import bindings as O
+    from slimtracincpp_b200 import layout as L
+    _, _, work = O.oracle_render(workload.scene, workload.projection(), workload.settings, workload.width,
+                                 workload.height, layout=L, count=True, threads=0)
+    return work["primary_rays"] + work["shadow_rays"] + work["bounce_rays"]
+
+
+def reference_frames(workload, seconds, min_frames=5, max_frames=200, threads=None):
+    """Whole frames of the reference's own CPU renderer (oracle/_ref, the
+    timing build) on the host cores, one warm-up frame, then frames until
+    `seconds` of wall time and at least `min_frames` are spent.  Returns the
+    per-frame seconds, the thread count and the build description."""
     from oracle import bindings as O
     from slimtracincpp_b200 import layout as L
     threads = threads or os.cpu_count() or 1
-    kind = "reference" if O.reference_available() else "port"
+    lib, build = O.reference_timed()
     proj = workload.projection()
-    h = workload.height
-    band = max(1, h // 36)
-    starts = list(range(0, h, band))
-    order = starts[::2] + starts[1::2]
-    band_rays = {}
-    rows_done, rays, t_total, frames = 0, 0, 0.0, 0
-    while t_total < seconds:
-        for r0 in order:
-            r1 = min(h, r0 + band)
-            t0 = time.perf_counter()
-            if kind == "reference":
-                O.reference_render(workload.scene, proj, workload.settings, workload.width, workload.height,
-                                   rows=(r0, r1), threads=threads, layout=L)
-            else:
-                O.oracle_render(workload.scene, proj, workload.settings, workload.width, workload.height,
-                                rows=(r0, r1), layout=L)
-            t_total += time.perf_counter() - t0
-            if r0 not in band_rays:
-                _, _, work = O.oracle_render(workload.scene, proj, workload.settings, workload.width, workload.height,
-                                             rows=(r0, r1), layout=L, count=True)
-                band_rays[r0] = work["primary_rays"] + work["shadow_rays"] + work["bounce_rays"]
-            rays += band_rays[r0]
-            rows_done += r1 - r0
-            if t_total >= seconds:
-                break
-        frames += 1
-    cores = threads if kind == "reference" else 1
-    return {"value": rays / t_total / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{rows_done} rows ({rows_done / h:.2f} frames, {rays} rays) of the {workload.width}x"
-                      f"{workload.height} frame rendered in {band}-row bands, {t_total:.2f} s wall on {cores} threads",
-            "seconds": t_total}
+    args = (workload.scene, proj, workload.settings, workload.width, workload.height)
+    O.reference_render(*args, threads=threads, layout=L, lib=lib)
+    times = []
+    while len(times) < max_frames and (len(times) < min_frames or sum(times) < seconds):
+        t0 = time.perf_counter()
+        O.reference_render(*args, threads=threads, layout=L, lib=lib)
+        times.append(time.perf_counter() - t0)
+    return times, threads, build
+
+
+def reference_one_core_frame(workload):
+    """One frame of the reference's unmodified single-threaded
+    RayTracingRenderer::renderOnCPU (renderer/renderer.h:87-100), timing
+    build; seconds."""
+    from oracle import bindings as O
+    from slimtracincpp_b200 import layout as L
+    lib, _ = O.reference_timed()
+    t0 = time.perf_counter()
+    O.reference_render_cpu(workload.scene, workload.projection(), workload.settings, workload.width, workload.height,
+                           layout=L, lib=lib)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(workload, seconds, rays=None):
+    """The reference's own CPU renderer (oracle/_ref) on all host cores:
+    whole frames of the same workload for about `seconds`, plus one frame of
+    its single-threaded renderOnCPU.  Ray counts come from the oracle."""
+    from oracle import bindings as O
+    kind = "reference" if O.reference_available() else "port"
+    rays = rays if rays is not None else frame_rays(workload)
+    if kind == "port":   # no reference build: the oracle itself, all cores
+        from slimtracincpp_b200 import layout as L
+        t0 = time.perf_counter()
+        O.oracle_render(workload.scene, workload.projection(), workload.settings, workload.width, workload.height,
+                        layout=L, threads=0)
+        dt = time.perf_counter() - t0
+        return {"value": rays / dt / 1e6, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
+                "sample": f"1 frame of {workload.width}x{workload.height} by the oracle port", "ms_per_frame": dt * 1e3,
+                "seconds": dt}
+    times, threads, build = reference_frames(workload, seconds)
+    med = statistics.median(times)
+    one = reference_one_core_frame(workload)
+    return {"value": rays / med / 1e6, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{len(times)} whole {workload.width}x{workload.height} frames ({rays} rays each) after 1 "
+                      f"warm-up frame, median frame time, {threads} threads claiming 4-row chunks; reference built {build}",
+            "ms_per_frame": med * 1e3, "frames": len(times),
+            "one_core": {"value": rays / one / 1e6, "unit": UNIT, "cores": 1, "ms_per_frame": one * 1e3,
+                         "sample": "1 frame of the unmodified single-threaded renderOnCPU (incremental directions)"},
+            "seconds": sum(times)}
+
+
+def native_libraries_loaded():
+    """Shared objects of this repository mapped into this process."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            path = line.split()[-1] if line.strip() else ""
+            if path.endswith(".so") and str(ROOT) in path:
+                out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 def run_reference(args):
+    """The reference's own CPU path on the host cores: the scene is built by
+    the reference's own code (mesh BVHs, scene BVH, camera projection from
+    oracle/_ref), then whole frames are rendered by its renderPixel on every
+    host thread; this process never loads libslimtracer_b200."""
     rank, world, _ = dist_info()
     if rank != 0:
         return 0
-    from slimtracincpp_b200 import scenes
     from oracle import bindings as O
-    w = scenes.CONFIGS[args.config](args.seed)
     if not O.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libslimref.so was not built"}))
         return 0
-    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
-    for _ in range(min(args.warmup, 1)):
-        cpu_baseline(w, 0.5)
-    vals = []
-    t0 = time.perf_counter()
+    if args.config in ("config3", "config5"):
+        print(json.dumps({"impl": "reference", "unavailable": f"{args.config}: the reference arm times config1, "
+                          "config2 and config4 (its textures would need this library's baker)"}))
+        return 0
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200 import scenes
+    from slimtracincpp_b200.scene import HOST_BUILDERS
+    HOST_BUILDERS.update(O.reference_host_builders(L))
+    w = scenes.CONFIGS[args.config](args.seed)
+    rays = frame_rays(w)
+    lib, build = O.reference_timed()
+    threads = os.cpu_count() or 1
+    proj = w.projection()
+    fargs = (w.scene, proj, w.settings, w.width, w.height)
+    for _ in range(max(1, min(args.warmup, 3))):
+        O.reference_render(*fargs, threads=threads, layout=L, lib=lib)
+    times = []
     for _ in range(args.steps):
-        vals.append(cpu_baseline(w, per_step))
-    wall = time.perf_counter() - t0
-    rays = sum(v["value"] * v["seconds"] for v in vals) * 1e6
-    secs = sum(v["seconds"] for v in vals)
-    value = rays / secs / 1e6
-    frame_rays = None
+        t0 = time.perf_counter()
+        O.reference_render(*fargs, threads=threads, layout=L, lib=lib)
+        times.append(time.perf_counter() - t0)
+    one = reference_one_core_frame(w)
+    total = sum(times)
+    value = rays * args.steps / total / 1e6
+    loaded = native_libraries_loaded()
+    assert not any("libslimtracer_b200" in p for p in loaded), loaded
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(1, args.steps), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": f"synthetic (seeded {args.config} scene)",
             "config": {"workload": w.name, "width": w.width, "height": w.height,
                        "max_depth": int(w.settings["max_depth"]), "geometries": len(w.scene.geometries),
-                       "triangles": sum(m.triangle_count for m in w.scene.meshes), "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": vals[0]["cores"], "kind": vals[0]["kind"],
-                             "sample": vals[0]["sample"]},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                       "triangles": sum(m.triangle_count for m in w.scene.meshes), "parallelism": "host threads",
+                       "rays_per_frame": rays},
+            "ms_per_frame": 1000.0 * statistics.median(times), "frame_ms": [1000.0 * t for t in times],
+            "one_core": {"value": rays / one / 1e6, "unit": UNIT, "cores": 1, "ms_per_frame": one * 1e3,
+                         "sample": "1 frame of the unmodified single-threaded renderOnCPU"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} whole frames ({rays} rays each), {threads} threads claiming 4-row chunks, "
+                                       f"scene built by the reference's own code; reference built {build}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_so_loaded": loaded}
     print(json.dumps(line))
     return 0
 

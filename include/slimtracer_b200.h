@@ -307,9 +307,16 @@ int slimRenderToDevice(const SlimCanvasData *canvas, const SlimCameraRayProjecti
  * several lights fits, 1080p does not) fail with SLIM_ERR_LIMIT.  The first
  * call on each device looks up the array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  Every call shares the one array: calls whose work overlaps on
- * the GPU (different streams, or threads without ordering) race and corrupt
- * each other's frames.  Debug render modes and max_depth 0 use no scratch. */
+ * capture, with the scene's device current (another current device is
+ * refused with SLIM_ERR_STATE).  Every call shares the one array: calls
+ * whose work overlaps on the GPU (different streams, or threads without
+ * ordering) race and corrupt each other's frames.  Debug render modes and
+ * max_depth 0 use no scratch and have no size limit.  The radiance cache and
+ * work counting are refused (SLIM_ERR_STATE): switch them off with
+ * slimSetRenderOptions first.  The call only enqueues work, so a device-side
+ * error of its kernels (a traversal stack overflow, say) is reported by the
+ * next synchronous call of the library (slimSynchronize, for one), as for
+ * slimRenderToDevice. */
 int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
                               const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths, void *stream);
 
@@ -355,6 +362,12 @@ int slimResetStageStats(void);
  * (GPU), keeping the topology last uploaded: scene/scene.h:165-191 rebuilds
  * it from scratch on the host every frame instead. */
 int slimRefitSceneBVH(void *stream);
+
+/* No counterpart in the reference (its scene BVH only lives on the host).
+ * Copies the device copy of the scene BVH -- as the last upload or refit
+ * left it -- into scene->bvh.nodes, whose node_count must equal the
+ * uploaded one.  Synchronous: waits for the last refit. */
+int slimDownloadSceneBVH(SlimSceneData *scene);
 
 /* ---- Neural radiance cache.  No counterpart in the reference. ----------
  * A 96-64-64-64-64-3 MLP (ReLU, exp output; bf16 weights and activations,

@@ -20,6 +20,10 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libslimref.so"
+# The reference built for timing: -O3 -DNDEBUG with the host's ISA level
+# (x86-64-v4 where the CPU has AVX-512, else x86-64-v3), no parity flags.
+REF_TIMED_LIBS = {"x86-64-v4": HERE / "_ref" / "libslimref_timed_v4.so",
+                  "x86-64-v3": HERE / "_ref" / "libslimref_timed_v3.so"}
 
 P = C.c_void_p
 WORK_FIELDS = ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests",
@@ -27,6 +31,7 @@ WORK_FIELDS = ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests",
 
 _oracle = None
 _ref = None
+_ref_timed = None
 
 
 def _ptr(a):
@@ -44,6 +49,8 @@ def oracle():
         h.oracle_render.restype = C.c_int
         h.oracle_trace_primary.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P]
         h.oracle_trace_primary.restype = C.c_int
+        h.oracle_trace_primary_rows.argtypes = [P, P, C.c_int, C.c_int, C.c_int, P, P, P, P]
+        h.oracle_trace_primary_rows.restype = C.c_int
         _oracle = h
     return _oracle
 
@@ -52,23 +59,79 @@ def reference_available():
     return REF_LIB.exists()
 
 
+def _bind_reference(path):
+    h = C.CDLL(str(path))
+    h.ref_projection_reset.argtypes = [P, P, C.c_float, C.c_int, C.c_int, C.c_int, P]
+    h.ref_build_scene_bvh.argtypes = [P]
+    h.ref_build_mesh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, P, P, P, P]
+    h.ref_render.argtypes = [P, P, P, P, C.c_int, C.c_int, C.c_int]
+    h.ref_render_cpu.argtypes = [P, P, P, P]
+    h.ref_trace_primary.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P, C.c_int]
+    for n in ["ref_projection_reset", "ref_build_scene_bvh", "ref_build_mesh", "ref_render", "ref_render_cpu",
+              "ref_trace_primary"]:
+        getattr(h, n).restype = C.c_int
+    return h
+
+
 def reference():
+    """The reference built with the parity flags (bit-exact checker)."""
     global _ref
     if _ref is None:
         if not REF_LIB.exists():
             raise FileNotFoundError(f"{REF_LIB} not built (oracle/build_ref.sh needs the reference sources)")
-        h = C.CDLL(str(REF_LIB))
-        h.ref_projection_reset.argtypes = [P, P, C.c_float, C.c_int, C.c_int, C.c_int, P]
-        h.ref_build_scene_bvh.argtypes = [P]
-        h.ref_build_mesh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, P, P, P, P]
-        h.ref_render.argtypes = [P, P, P, P, C.c_int, C.c_int, C.c_int]
-        h.ref_render_cpu.argtypes = [P, P, P, P]
-        h.ref_trace_primary.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P, C.c_int]
-        for n in ["ref_projection_reset", "ref_build_scene_bvh", "ref_build_mesh", "ref_render", "ref_render_cpu",
-                  "ref_trace_primary"]:
-            getattr(h, n).restype = C.c_int
-        _ref = h
+        _ref = _bind_reference(REF_LIB)
     return _ref
+
+
+def host_isa_level():
+    """x86-64-v4 when this CPU has the AVX-512 subsets that level requires,
+    else x86-64-v3 (AVX2 + FMA)."""
+    try:
+        flags = set()
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                flags = set(line.split(":", 1)[1].split())
+                break
+        if {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags:
+            return "x86-64-v4"
+    except OSError:
+        pass
+    return "x86-64-v3"
+
+
+def reference_timed():
+    """The reference built for timing (-O3 -DNDEBUG, the host's ISA level);
+    returns (library, description).  Falls back to the parity build when the
+    timing build is absent, and says so."""
+    global _ref_timed
+    if _ref_timed is None:
+        level = host_isa_level()
+        path = REF_TIMED_LIBS[level]
+        if path.exists():
+            _ref_timed = (_bind_reference(path), f"-O3 -DNDEBUG -march={level}")
+        else:
+            _ref_timed = (reference(), "parity build (-O3 -march=x86-64-v3 -ffp-contract=off): timing build absent")
+    return _ref_timed
+
+
+def reference_host_builders(layout, lib=None):
+    """Host builders for slimtracincpp_b200.scene.HOST_BUILDERS that run the
+    reference's own code (scene BVH, obj2mesh build, camera projection), so
+    a scene can be built without loading libslimtracer_b200."""
+    h = lib or reference()
+
+    def scene_bvh(sd):
+        rc = h.ref_build_scene_bvh(sd.ctypes.data)
+        assert rc == 0, rc
+
+    def mesh(pos, idx, nrm, nidx, uv, uidx):
+        tris, nodes, height, aabb, out_pos = reference_build_mesh(pos, idx, nrm, nidx, uv, uidx, layout=layout, lib=h)
+        return tris, nodes, height, aabb, out_pos
+
+    def projection(camera, width, height, ssaa):
+        return reference_projection(camera, width, height, ssaa, layout, lib=h)
+
+    return {"scene_bvh": scene_bvh, "mesh": mesh, "projection": projection}
 
 
 def make_canvas(width, height, antialias, layout):
@@ -88,33 +151,59 @@ def make_canvas(width, height, antialias, layout):
 
 
 def oracle_render(scene, projection, settings, width, height, antialias=0, rows=None, cones_per_pixel=False,
-                  count=False, layout=None):
-    """Renders with the C restatement; returns (pixels, depths, counters)."""
-    cv, pixels, depths = make_canvas(width, height, antialias, layout)
-    s = 2 if antialias == 2 else 1
-    r0, r1 = (0, height * s) if rows is None else rows
-    counters = np.zeros(10, np.uint64) if count else None
-    rc = oracle().oracle_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, int(cones_per_pixel),
-                                _ptr(counters))
-    assert rc == 0, rc
-    work = None if counters is None else dict(zip(WORK_FIELDS, (int(c) for c in counters)))
-    return pixels, depths, work
+                  count=False, layout=None, threads=1):
+    """Renders with the C restatement; returns (pixels, depths, counters).
 
-
-def reference_render(scene, projection, settings, width, height, antialias=0, rows=None, threads=None, layout=None):
+    threads > 1 (or 0: every host core) renders 8-row chunks of the rows on
+    that many host threads (ctypes releases the GIL around the call; the
+    oracle keeps all state per call and every pixel is written by the call
+    that owns its row), each with its own counters, summed at the end."""
     cv, pixels, depths = make_canvas(width, height, antialias, layout)
     s = 2 if antialias == 2 else 1
     r0, r1 = (0, height * s) if rows is None else rows
     threads = threads or os.cpu_count() or 1
-    rc = reference().ref_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, threads)
+    h = oracle()
+    if threads <= 1 or r1 - r0 <= 8:
+        counters = np.zeros(10, np.uint64) if count else None
+        rc = h.oracle_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, int(cones_per_pixel),
+                             _ptr(counters))
+        assert rc == 0, rc
+        work = None if counters is None else dict(zip(WORK_FIELDS, (int(c) for c in counters)))
+        return pixels, depths, work
+    from concurrent.futures import ThreadPoolExecutor
+    chunks = [(y, min(r1, y + 8)) for y in range(r0, r1, 8)]
+    per = [np.zeros(10, np.uint64) if count else None for _ in chunks]
+
+    def run(k):
+        a, b = chunks[k]
+        return h.oracle_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), a, b, int(cones_per_pixel),
+                               _ptr(per[k]))
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        rcs = list(ex.map(run, range(len(chunks))))
+    assert all(rc == 0 for rc in rcs), rcs
+    work = None
+    if count:
+        total = np.sum(np.stack(per), axis=0, dtype=np.uint64)
+        work = dict(zip(WORK_FIELDS, (int(c) for c in total)))
+    return pixels, depths, work
+
+
+def reference_render(scene, projection, settings, width, height, antialias=0, rows=None, threads=None, layout=None,
+                     lib=None):
+    cv, pixels, depths = make_canvas(width, height, antialias, layout)
+    s = 2 if antialias == 2 else 1
+    r0, r1 = (0, height * s) if rows is None else rows
+    threads = threads or os.cpu_count() or 1
+    rc = (lib or reference()).ref_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, threads)
     assert rc == 0, rc
     return pixels, depths
 
 
-def reference_render_cpu(scene, projection, settings, width, height, layout=None):
+def reference_render_cpu(scene, projection, settings, width, height, layout=None, lib=None):
     """The reference's unmodified single-threaded renderOnCPU."""
     cv, pixels, depths = make_canvas(width, height, 0, layout)
-    rc = reference().ref_render_cpu(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings))
+    rc = (lib or reference()).ref_render_cpu(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings))
     assert rc == 0, rc
     return pixels, depths
 
@@ -130,20 +219,37 @@ def _primary(fn, scene, projection, width, height, *extra):
     return g, p, d, b
 
 
-def oracle_trace_primary(scene, projection, width, height):
-    return _primary(oracle().oracle_trace_primary, scene, projection, width, height)
+def oracle_trace_primary(scene, projection, width, height, threads=1):
+    """Closest primary hits by the C restatement; threads > 1 (0: every host
+    core) traces 8-row chunks concurrently."""
+    threads = threads or os.cpu_count() or 1
+    if threads <= 1:
+        return _primary(oracle().oracle_trace_primary, scene, projection, width, height)
+    from concurrent.futures import ThreadPoolExecutor
+    n = width * height
+    g, p, d, b = np.zeros(n, np.int32), np.zeros(n, np.uint32), np.zeros(n, np.float32), np.zeros(n, np.uint8)
+    h = oracle()
+
+    def run(y):
+        return h.oracle_trace_primary_rows(scene.ptr, _ptr(projection), width, y, min(height, y + 8), _ptr(g), _ptr(p),
+                                           _ptr(d), _ptr(b))
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        rcs = list(ex.map(run, range(0, height, 8)))
+    assert all(rc == 0 for rc in rcs), rcs
+    return g, p, d, b
 
 
 def reference_trace_primary(scene, projection, width, height, threads=None):
     return _primary(reference().ref_trace_primary, scene, projection, width, height, threads or os.cpu_count() or 1)
 
 
-def reference_projection(camera, width, height, ssaa, layout):
+def reference_projection(camera, width, height, ssaa, layout, lib=None):
     out = np.zeros((), layout.PROJECTION)
     o = np.ascontiguousarray(camera.orientation, np.float32)
     p = np.ascontiguousarray(camera.position, np.float32)
-    rc = reference().ref_projection_reset(_ptr(o), _ptr(p), C.c_float(camera.focal_length), width, height, int(ssaa),
-                                          _ptr(out))
+    rc = (lib or reference()).ref_projection_reset(_ptr(o), _ptr(p), C.c_float(camera.focal_length), width, height,
+                                                   int(ssaa), _ptr(out))
     assert rc == 0
     return out
 
@@ -162,7 +268,7 @@ def reference_scene_bvh(scene, layout):
 
 
 def reference_build_mesh(positions, indices, normals=None, normal_indices=None, uvs=None, uv_indices=None,
-                         layout=None):
+                         layout=None, lib=None):
     pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
     idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
     t = len(idx)
@@ -176,7 +282,7 @@ def reference_build_mesh(positions, indices, normals=None, normal_indices=None, 
     ht = np.zeros(1, np.uint32)
     aabb = np.zeros(6, np.float32)
     out_pos = np.zeros_like(pos)
-    rc = reference().ref_build_mesh(_ptr(pos), len(pos), _ptr(idx), t, _ptr(nrm), 0 if nrm is None else len(nrm),
+    rc = (lib or reference()).ref_build_mesh(_ptr(pos), len(pos), _ptr(idx), t, _ptr(nrm), 0 if nrm is None else len(nrm),
                                     _ptr(nidx), _ptr(uv), 0 if uv is None else len(uv), _ptr(uidx), _ptr(tris),
                                     _ptr(nodes), _ptr(nc), _ptr(ht), _ptr(aabb), _ptr(out_pos))
     assert rc == 0

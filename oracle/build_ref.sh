@@ -29,6 +29,9 @@ if [ ! -d "$REF_SRC/slim" ]; then
     exit 2
 fi
 mkdir -p "$OUT"
+# Where the sources were read, for checks that read the reference's shipped
+# assets (examples/*.mesh, *.texture) in place.
+printf '%s\n' "$REF_SRC" > "$OUT/reference_src.txt"
 TMP="$(mktemp -d)"
 trap 'rm -rf "$TMP"' EXIT
 cp -r "$REF_SRC/slim" "$TMP/slim"
@@ -54,3 +57,16 @@ CXXFLAGS=(-std=c++17 -O3 -march=x86-64-v3 -mfma -ffp-contract=off -fno-fast-math
 g++ "${CXXFLAGS[@]}" -shared -o "$OUT/libslimref.so.tmp" "$HERE/ref/ref_driver.cpp"
 mv "$OUT/libslimref.so.tmp" "$OUT/libslimref.so"
 echo "built $OUT/libslimref.so"
+
+# The timed CPU baseline: the same sources with plain release flags
+# (-O3 -DNDEBUG, the compiler's default contraction, no parity flags).  The
+# GPU host that times it may be another CPU than this build machine, so
+# instead of -march=native there is one build per ISA level and the timing
+# code loads the one the host supports: x86-64-v4 (AVX-512) and x86-64-v3
+# (AVX2 + FMA).
+for LEVEL in v3 v4; do
+    g++ -std=c++17 -O3 -DNDEBUG -march=x86-64-$LEVEL -fPIC -pthread -w -include "$HERE/ref/ref_shim.h" -I "$TMP" \
+        -shared -o "$OUT/libslimref_timed_$LEVEL.so.tmp" "$HERE/ref/ref_driver.cpp"
+    mv "$OUT/libslimref_timed_$LEVEL.so.tmp" "$OUT/libslimref_timed_$LEVEL.so"
+    echo "built $OUT/libslimref_timed_$LEVEL.so"
+done

@@ -22,6 +22,7 @@
  *   ref_trace_primary     SceneTracer::trace of each primary ray
  *                         (renderer/ray_tracer.h:36-45, scene/scene_tracer.h:26-98)
  */
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -103,16 +104,34 @@ struct PixelContext {
     }
 };
 
+// Runs fn(y0, y1) over [0, rows) on `threads` host threads.  Rows are
+// claimed dynamically in chunks of 4 (an atomic counter), so threads whose
+// rows are cheap (sky) take more of them and the frame ends when the work
+// does, not when the most expensive static band does.
+// A zeroed context: the reference app's tracer stacks come from zeroed
+// pages (os::getMemory), and its traversal may read a stack slot it has not
+// written in this pixel, so they must start as zero here too.
+PixelContext *new_context() {
+    PixelContext *ctx = (PixelContext*)aligned_alloc(64, sizeof(PixelContext));
+    if (ctx) memset((void*)ctx, 0, sizeof(PixelContext));
+    return ctx;
+}
+
 template <typename Fn>
 void parallel_rows(int rows, int threads, Fn fn) {
     if (threads <= 1) { fn(0, rows); return; }
+    constexpr int kChunk = 4;
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            int y0 = next.fetch_add(kChunk);
+            if (y0 >= rows) break;
+            fn(y0, y0 + kChunk < rows ? y0 + kChunk : rows);
+        }
+    };
     std::vector<std::thread> pool;
-    int band = (rows + threads - 1) / threads;
-    for (int t = 0; t < threads; t++) {
-        int y0 = t * band, y1 = y0 + band < rows ? y0 + band : rows;
-        if (y0 >= y1) break;
-        pool.emplace_back([=]() { fn(y0, y1); });
-    }
+    for (int t = 1; t < threads; t++) pool.emplace_back(worker);
+    worker();
     for (auto &th : pool) th.join();
 }
 }  // namespace
@@ -260,7 +279,7 @@ int ref_render(const void *scene_data, const void *canvas_data, const void *proj
     if (row_begin < 0) row_begin = 0;
     if (row_begin >= row_end) return 0;
     parallel_rows(row_end - row_begin, threads, [&](int y0, int y1) {
-        PixelContext *ctx = (PixelContext*)aligned_alloc(64, sizeof(PixelContext));
+        PixelContext *ctx = new_context();
         Color color;
         f32 depth;
         for (i32 y = row_begin + y0; y < row_begin + y1; y++)
@@ -289,7 +308,7 @@ int ref_render_cpu(const void *scene_data, const void *canvas_data, const void *
     const Canvas &canvas = *(const Canvas*)canvas_data;
     CameraRayProjection projection = *(const CameraRayProjection*)projection_data;
     const RayTracerSettings &settings = *(const RayTracerSettings*)settings_data;
-    PixelContext *ctx = (PixelContext*)aligned_alloc(64, sizeof(PixelContext));
+    PixelContext *ctx = new_context();
     ctx->fresh();
     void *renderer_mem = calloc(1, sizeof(RayTracingRenderer));
     RayTracingRenderer *renderer = new (renderer_mem) RayTracingRenderer{
@@ -313,7 +332,7 @@ int ref_trace_primary(const void *scene_data, const void *projection_data, int w
     const Scene &scene = *(const Scene*)scene_data;
     const CameraRayProjection &projection = *(const CameraRayProjection*)projection_data;
     parallel_rows(height, threads, [&](int y0, int y1) {
-        PixelContext *ctx = (PixelContext*)aligned_alloc(64, sizeof(PixelContext));
+        PixelContext *ctx = new_context();
         for (i32 y = y0; y < y1; y++)
             for (i32 x = 0; x < width; x++) {
                 ctx->fresh();

@@ -1032,16 +1032,18 @@ int oracle_render(const SlimSceneData *scene, const SlimCanvasData *canvas, cons
     return SLIM_OK;
 }
 
-/* First closest hit of each primary ray (renderer/ray_tracer.h:36-45). */
-int oracle_trace_primary(const SlimSceneData *scene, const SlimCameraRayProjection *proj, int width, int height,
-                         int32_t *geometry_ids, uint32_t *primitive_ids, float *distances, uint8_t *from_behind) {
+/* First closest hit of each primary ray (renderer/ray_tracer.h:36-45) of
+ * rows [row_begin, row_end); outputs are indexed y * width + x. */
+int oracle_trace_primary_rows(const SlimSceneData *scene, const SlimCameraRayProjection *proj, int width,
+                              int row_begin, int row_end, int32_t *geometry_ids, uint32_t *primitive_ids,
+                              float *distances, uint8_t *from_behind) {
     Tracer *tr = (Tracer*)calloc(1, sizeof(Tracer));
     if (!tr) return SLIM_ERR_LIMIT;
     v3 start = V3(proj->start.x, proj->start.y, proj->start.z);
     v3 down = V3(proj->down.x, proj->down.y, proj->down.z);
     v3 right = V3(proj->right.x, proj->right.y, proj->right.z);
     v3 cam = V3(proj->camera_position.x, proj->camera_position.y, proj->camera_position.z);
-    for (int y = 0; y < height; y++)
+    for (int y = row_begin; y < row_end; y++)
         for (int x = 0; x < width; x++) {
             Ray ray; Hit hit;
             memset(tr, 0, sizeof(Tracer)); memset(&ray, 0, sizeof(ray)); memset(&hit, 0, sizeof(hit));
@@ -1056,4 +1058,10 @@ int oracle_trace_primary(const SlimSceneData *scene, const SlimCameraRayProjecti
         }
     free(tr);
     return SLIM_OK;
+}
+
+int oracle_trace_primary(const SlimSceneData *scene, const SlimCameraRayProjection *proj, int width, int height,
+                         int32_t *geometry_ids, uint32_t *primitive_ids, float *distances, uint8_t *from_behind) {
+    return oracle_trace_primary_rows(scene, proj, width, 0, height, geometry_ids, primitive_ids, distances,
+                                     from_behind);
 }

@@ -117,7 +117,8 @@ def build_reference(verbose: bool = False):
     present (they are only on the development machine); returns the library
     path or None."""
     script = ROOT / "oracle" / "build_ref.sh"
-    if not Path("/root/reference/src/slim").is_dir() and not os.environ.get("SLIM_REFERENCE_SRC"):
+    src = Path(os.environ.get("SLIM_REFERENCE_SRC", "/root/reference/src"))
+    if not (src / "slim").is_dir():
         lib = ROOT / "oracle" / "_ref" / "libslimref.so"
         return lib if lib.exists() else None
     _run(["bash", script], verbose)

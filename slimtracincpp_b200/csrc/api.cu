@@ -1054,6 +1054,9 @@ using namespace slim;
 // A batch's tables point into the shared mesh and texture arrays and its
 // graph into the cache's weights: re-initialising either drops the batch.
 static void invalidate_batch();
+// Forgets the cached device addresses of the no-alloc scratch (looked up
+// again by the next no-alloc call).
+static void noalloc_forget();
 
 extern "C" {
 
@@ -1066,6 +1069,7 @@ int slimInitDataOnGPU(const SlimSceneData *scene) {
     int rc = ensure_device(c);
     if (rc) return rc;
     invalidate_batch();
+    noalloc_forget();
     if ((rc = check_scene_arrays(scene))) return rc;
     c.initialized = false;
     c.counts = scene->counts;
@@ -1255,6 +1259,19 @@ int slimGetWorkCounters(SlimWorkCounters *counters) {
     return SLIM_OK;
 }
 
+int slimDownloadSceneBVH(SlimSceneData *scene) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!scene || !scene->bvh.nodes) return set_error(SLIM_ERR_ARGUMENT, "slimDownloadSceneBVH: null argument");
+    if (scene->bvh.node_count != c.scene_node_count)
+        return set_error(SLIM_ERR_STATE, "scene BVH node count differs from the uploaded one");
+    if (c.refit_done) SLIM_CUDA(cudaEventSynchronize(c.refit_done), "wait for the refit");
+    SLIM_CUDA(cudaMemcpy(scene->bvh.nodes, c.d_scene_nodes.ptr, c.scene_node_count * sizeof(SlimBVHNode),
+                         cudaMemcpyDeviceToHost), "download scene BVH");
+    return SLIM_OK;
+}
+
 int slimRefitSceneBVH(void *stream) {
     std::lock_guard<std::mutex> lock(g_mutex);
     Context &c = g_ctx;
@@ -1361,10 +1378,13 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 unsigned char *g_noalloc_base[kNoAllocMaxDevices] = {};
 
 // Device address of this device's copy of the array, looked up once per
-// device (host code may only use the symbol through this address).
-int noalloc_scratch(unsigned char **out) {
+// device (host code may only use the symbol through this address).  The
+// calling thread's current device must be the one that holds the scene.
+int noalloc_scratch(int scene_device, unsigned char **out) {
     int device = 0;
     SLIM_CUDA(cudaGetDevice(&device), "cudaGetDevice");
+    if (device != scene_device)
+        return set_error(SLIM_ERR_STATE, "slimRenderToDeviceNoAlloc: the current device is not the scene's device");
     if (device < 0 || device >= kNoAllocMaxDevices) return set_error(SLIM_ERR_LIMIT, "device index beyond 64");
     if (!g_noalloc_base[device]) {
         void *p = nullptr;
@@ -1411,6 +1431,10 @@ int noalloc_layout(unsigned char *base, uint32_t samples, uint32_t lights, Wavef
 }  // namespace
 }  // namespace slim
 
+static void noalloc_forget() {
+    for (int i = 0; i < slim::kNoAllocMaxDevices; i++) slim::g_noalloc_base[i] = nullptr;
+}
+
 extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
                                          const SlimRayTracerSettings *settings, void *d_pixels, void *d_depths,
                                          void *stream) {
@@ -1440,14 +1464,25 @@ extern "C" int slimRenderToDeviceNoAlloc(const SlimCanvasData *canvas, const Sli
     F.depths = (float *)d_depths;
     F.error_flags = c.d_error.ptr;
     F.counters = nullptr;
-    unsigned char *scratch = nullptr;
-    if ((rc = noalloc_scratch(&scratch))) return rc;
+    // The radiance cache keeps per-frame state and buffers of its own, and
+    // work counting reads back device counters: neither fits a call that
+    // allocates nothing, so both are refused rather than ignored.
+    if (c.options.radiance_cache != SLIM_CACHE_OFF)
+        return set_error(SLIM_ERR_STATE, "slimRenderToDeviceNoAlloc: the radiance cache is on");
+    if (c.options.count_work)
+        return set_error(SLIM_ERR_STATE, "slimRenderToDeviceNoAlloc: work counting is on");
     WavefrontBuffers B;
     memset(&B, 0, sizeof(B));
-    if ((rc = noalloc_layout(scratch, F.width * F.rows, c.scene.light_count, B))) return rc;
-    // The queue counters at the head of the scratch are zeroed by the
-    // launcher (cudaMemsetAsync) before the first stage reads them; every
-    // other region is written before it is read within the frame.
+    // Debug render modes and max_depth 0 go to the fused kernel, which
+    // queues nothing: no scratch, so no size limit either.
+    if (settings->render_mode == SLIM_RENDER_BEAUTY && settings->max_depth != 0) {
+        unsigned char *scratch = nullptr;
+        if ((rc = noalloc_scratch(c.device, &scratch))) return rc;
+        if ((rc = noalloc_layout(scratch, F.width * F.rows, c.scene.light_count, B))) return rc;
+    }
+    // The queue counters (after the per-sample arrays in the scratch) are
+    // zeroed by the launcher (cudaMemsetAsync) before the first stage reads
+    // them; every other region is written before it is read within the frame.
     if ((rc = wait_for_refit(c, (cudaStream_t)stream))) return rc;
     cudaError_t e = launch_render_wavefront(c.scene, F, B, c.options.block_size, (cudaStream_t)stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "no-alloc render launch");

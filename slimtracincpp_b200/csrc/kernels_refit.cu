@@ -3,7 +3,7 @@
 // every frame (scene/scene.h:176-191); a refit keeps the uploaded topology
 // and recomputes every node's bounds: leaves from their geometry's world
 // AABB (Scene::updateAABB, scene/scene.h:165-174), inner nodes as the union
-// of their two children (AABB::operator+, math/vec3.h:436-445).
+// of their two children (AABB::operator+, math/vec3.h:471-480).
 #include "kernels.h"
 #include "tracer_core.cuh"
 
@@ -28,8 +28,11 @@ SLIM_D void world_box(const DevScene &S, uint32_t gi, float mn[3], float mx[3]) 
             for (int k = 0; k < 2; k++) {
                 float3 p = f3(i ? hi[0] : lo[0], j ? hi[1] : lo[1], k ? hi[2] : lo[2]);
                 p = qrot(g.axis, g.w, g.s * p) + g.p;
-                mn[0] = p.x < mn[0] ? p.x : mn[0]; mn[1] = p.y < mn[1] ? p.y : mn[1]; mn[2] = p.z < mn[2] ? p.z : mn[2];
-                mx[0] = p.x > mx[0] ? p.x : mx[0]; mx[1] = p.y > mx[1] ? p.y : mx[1]; mx[2] = p.z > mx[2] ? p.z : mx[2];
+                // minimum(min, pos) / maximum(max, pos) (math/vec3.h:403-417):
+                // the running bound is the first operand, so an equal pair
+                // (+0 against -0) keeps the corner's sign as the reference does
+                mn[0] = mn[0] < p.x ? mn[0] : p.x; mn[1] = mn[1] < p.y ? mn[1] : p.y; mn[2] = mn[2] < p.z ? mn[2] : p.z;
+                mx[0] = mx[0] > p.x ? mx[0] : p.x; mx[1] = mx[1] > p.y ? mx[1] : p.y; mx[2] = mx[2] > p.z ? mx[2] : p.z;
             }
 }
 

@@ -30,7 +30,7 @@ EXPORTS = [
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
     "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimSynchronize",
-    "slimGetLaunchCount", "slimPick",
+    "slimGetLaunchCount", "slimPick", "slimDownloadSceneBVH",
     "slimBatchSetRequests", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender",
 ]
 
@@ -59,7 +59,7 @@ def lib():
     h.slimGetLastError.argtypes = []
     for name in ["slimInitDataOnGPU", "slimUploadLights", "slimUploadCameras", "slimUploadGeometries",
                  "slimUploadMaterials", "slimUploadSceneBVH", "slimBuildSceneBVH", "slimSetRenderOptions",
-                 "slimGetRenderOptions", "slimGetWorkCounters", "slimRefitSceneBVH"]:
+                 "slimGetRenderOptions", "slimGetWorkCounters", "slimRefitSceneBVH", "slimDownloadSceneBVH"]:
         getattr(h, name).argtypes = [P]
         getattr(h, name).restype = C.c_int
     h.slimRenderOnGPU.argtypes = [P, P, P]

@@ -10,6 +10,16 @@ import numpy as np
 from . import layout as L
 from .native import check, lib, ptr
 
+# Host-side builders the containers below call: the library's own
+# restatements by default.  A caller may put other implementations of the
+# same algorithms here (same arguments, same outputs), e.g. to build a scene
+# for another renderer without loading this library:
+#   "scene_bvh"   f(scene_data_record)          Scene::updateAABBs + updateBVH
+#   "mesh"        f(positions, indices, normals, normal_indices, uvs, uv_indices)
+#                   -> (triangles, nodes, height, aabb6, recentred positions)
+#   "projection"  f(camera, width, height, ssaa) -> CameraRayProjection record
+HOST_BUILDERS = {}
+
 
 class MeshAsset:
     """A mesh with its leaf-ordered Triangle records and SAH BVH, as the
@@ -45,6 +55,9 @@ class MeshAsset:
         nidx = None if normal_indices is None else np.ascontiguousarray(normal_indices, np.uint32).reshape(-1, 3)
         uv = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
         uidx = None if uv_indices is None else np.ascontiguousarray(uv_indices, np.uint32).reshape(-1, 3)
+        if "mesh" in HOST_BUILDERS:
+            tris, nodes, height, aabb, pos = HOST_BUILDERS["mesh"](pos, idx, nrm, nidx, uv, uidx)
+            return cls(tris, nodes, aabb[:3], aabb[3:], height, pos, idx, nrm, nidx, uv, uidx, _edges(idx))
         tris = np.zeros(t, L.TRIANGLE)
         nodes = np.zeros(2 * t, L.BVH_NODE)
         node_count = np.zeros(1, np.uint32)
@@ -196,6 +209,8 @@ class Camera:
         return cls(np.concatenate([right, up, fwd]).astype(np.float32), p.astype(np.float32), focal)
 
     def projection(self, width, height, ssaa=False):
+        if "projection" in HOST_BUILDERS:
+            return HOST_BUILDERS["projection"](self, width, height, ssaa)
         from .native import projection_reset
         return projection_reset(self.orientation, self.position, self.focal_length, width, height, ssaa)
 
@@ -242,6 +257,9 @@ class Scene:
 
     def build_bvh(self):
         """Scene::updateAABBs + updateBVH (scene/scene.h:176-191) on the host."""
+        if "scene_bvh" in HOST_BUILDERS:
+            HOST_BUILDERS["scene_bvh"](self.data)
+            return
         check(lib().slimBuildSceneBVH(ptr(self.data)))
 
     @property

@@ -107,7 +107,13 @@ def heightfield(rng, n=256, amplitude=0.3):
 
 
 def cached_mesh(name, builder):
-    """Builds a mesh asset once per machine and reuses its .mesh file."""
+    """Builds a mesh asset once per machine and reuses its .mesh file (read
+    and written by this library; a caller-supplied mesh builder builds it
+    afresh instead)."""
+    from .scene import HOST_BUILDERS
+    if "mesh" in HOST_BUILDERS:
+        pos, idx, nrm = builder()
+        return MeshAsset.build(pos, idx, normals=nrm, normal_indices=idx)
     ASSET_CACHE.mkdir(parents=True, exist_ok=True)
     path = ASSET_CACHE / f"{name}.mesh"
     if path.exists():

@@ -28,3 +28,14 @@ def gpu_available():
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def reference_src():
+    """The reference's source tree, for checks that read its shipped assets
+    in place: $SLIM_REFERENCE_SRC, else the tree oracle/build_ref.sh read
+    (recorded in oracle/_ref/reference_src.txt); None when neither exists."""
+    cand = os.environ.get("SLIM_REFERENCE_SRC")
+    rec = ROOT / "oracle" / "_ref" / "reference_src.txt"
+    if not cand and rec.exists():
+        cand = rec.read_text().strip()
+    return Path(cand) if cand and Path(cand).is_dir() else None

@@ -131,3 +131,39 @@ def test_cache_requests_in_a_batch(meshes):
             b = RayTracingRenderer.to_content(spix, q.width, q.height).astype(np.float64)
             mse = np.mean((a - b) ** 2)
             assert mse == 0 or 10 * np.log10(255.0 ** 2 / mse) > 20.0, q.name
+
+
+def _assert_matches_oracle(q, pix, dep):
+    from oracle import bindings as O
+    opix, odep, _ = O.oracle_render(q.scene, q.projection(), q.settings, q.width, q.height, layout=L, threads=0)
+    a = RayTracingRenderer.to_content(pix, q.width, q.height).astype(np.int32)
+    b = RayTracingRenderer.to_content(opix, q.width, q.height).astype(np.int32)
+    within = (np.abs(a - b) <= 1).all(axis=-1).mean()
+    assert within >= 0.999, f"{q.name}: only {within:.5f} of pixels within 1 LSB of the oracle"
+    finite = np.isfinite(odep)
+    assert np.array_equal(np.isfinite(dep), finite), q.name
+    np.testing.assert_allclose(dep[finite], odep[finite], rtol=1e-5, atol=0, err_msg=q.name)
+
+
+def test_batch_matches_oracle(meshes):
+    """Every request of a batch against the CPU oracle on its own scene (the
+    reference's per-pixel path, renderer/ray_tracer.h:144-161): 8-bit pixels
+    within 1 LSB on >= 99.9% of pixels, depths within 1e-5 relative."""
+    reqs = make_requests(meshes, 4, 8)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    got = render_batch(BatchRenderer(assets(meshes)), reqs, plan=(1 << 16, 4096, 256))
+    for q, (pix, dep) in zip(reqs, got):
+        _assert_matches_oracle(q, pix, dep)
+
+
+def test_config5_shaped_batch_matches_oracle():
+    """config 5's request generator with the full config-2 meshes (81,920
+    and 130,050 triangles), at the two smallest resolutions; the requests
+    without the radiance cache are checked against the oracle."""
+    mesh_assets = scenes.config2_meshes()
+    reqs = scenes.config5(5, count=8, meshes=mesh_assets, resolutions=[(320, 180), (640, 360)])
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    plain = [q for q in reqs if q.radiance_cache == L.CACHE_OFF]
+    got = render_batch(BatchRenderer(assets(mesh_assets)), plain)
+    for q, (pix, dep) in zip(plain, got):
+        _assert_matches_oracle(q, pix, dep)

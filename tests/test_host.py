@@ -13,6 +13,7 @@ from slimtracincpp_b200 import layout as L
 from slimtracincpp_b200 import native, scenes
 from slimtracincpp_b200.scene import Camera, MeshAsset, Scene, geometry
 from oracle import bindings as O
+from conftest import reference_src
 
 ROOT = Path(__file__).resolve().parent.parent
 GOLDEN = ROOT / "tests" / "golden"
@@ -151,7 +152,8 @@ def test_mesh_file_truncated_is_an_io_error(tmp_path):
 def test_shipped_reference_meshes_load():
     """monkey.mesh / cube.mesh from the reference's examples (read in place
     when the reference sources are present)."""
-    ex = Path("/root/reference/src/examples")
+    src = reference_src()
+    ex = src / "examples" if src else Path("/nonexistent")
     if not (ex / "monkey.mesh").exists():
         pytest.skip("reference assets not present")
     monkey = MeshAsset.load(ex / "monkey.mesh")
@@ -200,7 +202,8 @@ def test_texture_baker_reproduces_shipped_reference_textures(name, tmp_path):
     """The reference ships these cube maps baked by its bmp2texture -c -l
     from the BMPs beside them; the restated baker must write the same bytes."""
     from slimtracincpp_b200.scene import TextureAsset
-    ex = Path("/root/reference/src/examples")
+    src = reference_src()
+    ex = src / "examples" if src else Path("/nonexistent")
     if not (ex / f"{name}.texture").exists():
         pytest.skip("reference assets not present")
     t = TextureAsset.bake(_load_bmp_components(ex / f"{name}.bmp"), L.IMAGE_CUBEMAP | L.IMAGE_LINEAR)

@@ -59,7 +59,12 @@ def parse():
                         "captures of whole-frame launches)")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     p.add_argument("--train-samples", type=int, default=65536,
-                   help="radiance cache (config4): training paths per frame, each traced to full depth")
+                   help="radiance cache (config4): training paths per frame")
+    p.add_argument("--train-suffix", type=int, default=0,
+                   help="radiance cache (config4): 0 = training paths traced to full depth (as specified); k = "
+                        "traced k bounces past the cache vertex into the cache's own answer")
+    p.add_argument("--no-cache-block", action="store_true",
+                   help="default workload: skip the radiance-cache comparison block")
     return p.parse_args()
 
 
@@ -364,6 +369,43 @@ def run_reference(args):
 NRC_FLOPS_PER_QUERY = 2 * (96 * 64 + 3 * 64 * 64 + 64 * 16)   # tensor-core MACs x 2 (output padded to 16)
 
 
+def nrc_roofline(torch, native, w, dev, frames=4):
+    """Tensor-pipe roofline of the cache's query kernel (k_nrc_infer): the
+    network's flops per launch over its CUDA-event time, a few cache frames
+    with per-stage events (the cache keeps its trained weights)."""
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200.radiance_cache import RadianceCache
+    from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport
+    r = RayTracingRenderer(w.scene, 8)
+    vp = Viewport(w.camera, w.width, w.height)
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    pix = torch.empty((w.samples, 4), dtype=torch.float32, device=dev)
+    dep = torch.empty(w.samples, dtype=torch.float32, device=dev)
+    RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=0)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON, profile_stages=True)
+    for _ in range(2):
+        r.render_to_device(vp, pix.data_ptr(), dep.data_ptr(), sp)
+    torch.cuda.synchronize()
+    native.reset_stage_stats()
+    for _ in range(frames):
+        r.render_to_device(vp, pix.data_ptr(), dep.data_ptr(), sp)
+    RadianceCache().join(sp)
+    torch.cuda.synchronize()
+    stats = {s["name"]: s for s in native.stage_stats()}
+    queries = RadianceCache().stats()["queries"]
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    q = stats.get("cache_query")
+    if not q or not q["launches"]:
+        return None
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak_tf = float(peaks.get("bf16_tflops", 1590.0))
+    ms = q["total_ms"] / q["launches"]
+    ach = queries * NRC_FLOPS_PER_QUERY / (ms / 1000.0) / 1e12
+    return {"kernel": "k_nrc_infer", "bound": "tensor", "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": ach / peak_tf, "flops_per_query": NRC_FLOPS_PER_QUERY, "queries": queries, "ms_per_launch": ms,
+            "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops)" if peaks else "fallback 1590 TFLOP/s"}
+
+
 def timed_frames(torch, native, r, vp, sp, stream, outputs, flush):
     """One device-resident frame (scene refit + render) per entry of
     `outputs` (pixel, depth tensors), L2 flushed before each, timed with
@@ -381,26 +423,42 @@ def timed_frames(torch, native, r, vp, sp, stream, outputs, flush):
     return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
 
-def run_cache_bench(args, torch, dist, dev, rank, world, local):
-    """Config 4: the config-2 scene at bounce depth 8.  Plain wavefront frames
-    against radiance-cache frames (paths stop at vertex 2, 65,536 training
-    paths and four Adam steps of 16,384 per frame, then the cache answers
-    every query); every timed cache frame is scored against the plain
-    depth-8 frame (PSNR of the 8-bit canvas, max abs of the stored values)."""
+def frame_quality(pix, ref_pix):
+    """PSNR of the 8-bit canvas and max abs error of the stored colours
+    against the reference frame (the plain depth-8 frame)."""
+    ref8 = torch_floor8(ref_pix)
+    p8 = torch_floor8(pix)
+    mse = float(((p8 - ref8) ** 2).mean())
+    psnr = 99.0 if mse == 0 else 10.0 * float(np.log10(255.0 ** 2 / mse))
+    return psnr, float((pix[:, :3] - ref_pix[:, :3]).abs().max())
+
+
+def torch_floor8(pix):
+    import torch
+    return torch.floor(255.0 * torch.sqrt(pix[:, :3].clamp(0, 1)))
+
+
+def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffixes, seed=0):
+    """Config 4 (config 2's scene at bounce depth 8): plain wavefront
+    frames against radiance-cache frames (paths stop at vertex 2; each frame
+    trains on `train_samples` paths with four Adam steps of 16,384, then the
+    cache answers every query).  For every training suffix in `suffixes` (0:
+    full-depth training paths, as specified; k: self-training k bounces into
+    the cache's own answers) the cache starts from fresh weights, learns
+    online for max(warmup, 16) frames, then `steps` frames are timed back to
+    back (the span from the first frame's start to the join of the last
+    frame's overlapped training) and each is scored against the plain
+    depth-8 frame."""
     from slimtracincpp_b200 import layout as L
-    from slimtracincpp_b200 import native, scenes
     from slimtracincpp_b200.radiance_cache import RadianceCache
-    from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport, make_canvas
-    w = scenes.config4(args.seed)
+    from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport
     lib = native.lib()
-    st = w.settings
-    r = RayTracingRenderer(w.scene, int(st["max_depth"]))
+    r = RayTracingRenderer(w.scene, 8)
     vp = Viewport(w.camera, w.width, w.height)
     n = w.samples
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    steps = args.steps
 
     def buffers(k):
         return [(torch.empty((n, 4), dtype=torch.float32, device=dev), torch.empty(n, dtype=torch.float32, device=dev))
@@ -415,65 +473,82 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
         wk = native.work_counters()
         return wk["primary_rays"] + wk["shadow_rays"] + wk["bounce_rays"]
 
-    # plain depth-8 frames: timing and the reference image
     plain_rays = counted(L.CACHE_OFF)
-    native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
     ref = buffers(1)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         native.check(lib.slimRefitSceneBVH(sp))
         r.render_to_device(vp, ref[0][0].data_ptr(), ref[0][1].data_ptr(), sp)
-    native.reset_stage_stats()
     plain_ms = timed_frames(torch, native, r, vp, sp, stream, ref * steps, flush)
-    plain_stages = {s["name"]: s["total_ms"] / steps for s in native.stage_stats() if s["launches"]}
+    out = {"plain_depth8": {"ms_per_frame": sum(plain_ms) / steps, "rays_per_frame": plain_rays,
+                            "mrays_s": plain_rays / (sum(plain_ms) / steps / 1000.0) / 1e6}, "cache": []}
+    cache_warmup = max(warmup, CACHE_WARMUP_FRAMES)
+    for suffix in suffixes:
+        cache = RadianceCache.configure(cache_depth=2, train_samples=train_samples, batch=16384, seed=seed,
+                                        train_suffix=suffix)
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
+        outs = buffers(steps)
+        for _ in range(cache_warmup):
+            native.check(lib.slimRefitSceneBVH(sp))
+            r.render_to_device(vp, outs[0][0].data_ptr(), outs[0][1].data_ptr(), sp)
+        cache.join(sp)
+        torch.cuda.synchronize()
+        t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        launches0 = native.launch_count()
+        frame_ms = timed_frames(torch, native, r, vp, sp, stream, outs, flush)
+        launches = native.launch_count() - launches0
+        cache.join(sp)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        total = t_start.elapsed_time(t_end)
+        quality = [frame_quality(p, ref[0][0]) for p, _ in outs]
+        rays = counted(L.CACHE_ON)
+        cst = cache.stats()
+        out["cache"].append({
+            "train_targets": "full-depth paths traced by the tracer (as specified)" if suffix == 0 else
+                             f"self-training: {suffix} bounce(s) past the cache vertex, then the cache's own answer",
+            "train_suffix": suffix, "ms_per_frame": total / steps, "rays_per_frame": rays,
+            "speedup_vs_plain_depth8": (sum(plain_ms) / steps) / (total / steps),
+            "psnr_db_per_frame": [q[0] for q in quality], "max_abs_per_frame": [q[1] for q in quality],
+            "min_psnr_db": min(q[0] for q in quality), "frame_event_ms": frame_ms,
+            "cache_warmup_frames": cache_warmup, "gpu_launches": launches,
+            "queries": cst["queries"], "train_samples": cst["train_samples"], "loss": cst["loss"]})
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    return out
 
-    # radiance-cache frames (online training continues through warm-up and timing)
-    cache = RadianceCache.configure(cache_depth=2, train_samples=args.train_samples, batch=16384, seed=args.seed)
-    native.set_render_options(engine=L.ENGINE_WAVEFRONT, profile_stages=True, radiance_cache=L.CACHE_ON)
-    outs = buffers(steps)
-    # the cache learns online: its first frames are its warm-up (at least
-    # CACHE_WARMUP_FRAMES frames, or the bench's warm-up count if larger)
-    cache_warmup = max(args.warmup, CACHE_WARMUP_FRAMES)
-    for _ in range(cache_warmup):
-        native.check(lib.slimRefitSceneBVH(sp))
-        r.render_to_device(vp, outs[0][0].data_ptr(), outs[0][1].data_ptr(), sp)
-    cache.join(sp)
-    torch.cuda.synchronize()
-    native.reset_stage_stats()
+
+def run_cache_bench(args, torch, dist, dev, rank, world, local):
+    """Config 4: the config-2 scene at bounce depth 8.  Plain wavefront frames
+    against radiance-cache frames (paths stop at vertex 2, 65,536 training
+    paths and four Adam steps of 16,384 per frame, then the cache answers
+    every query); every timed cache frame is scored against the plain
+    depth-8 frame (PSNR of the 8-bit canvas, max abs of the stored values).
+    `--train-suffix k` trains on paths that end in the cache's own answer k
+    bounces past the cache vertex instead of full-depth paths."""
+    from slimtracincpp_b200 import layout as L
+    from slimtracincpp_b200 import native, scenes
+    from slimtracincpp_b200.radiance_cache import RadianceCache
+    from slimtracincpp_b200.renderer import RayTracingRenderer, make_canvas
+    w = scenes.config4(args.seed)
+    lib = native.lib()
+    n = w.samples
+    steps = args.steps
     clocks = ClockSampler(local, device_uuid(dev))
     clocks.start()
     if world > 1:
         dist.barrier()
-    torch.cuda.synchronize()
-    # Frames back to back; the cache trains each frame's paths on its second
-    # stream while the next frame runs, so the span from the first frame's
-    # start to the join of the last frame's training is the honest total.
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    launches0 = native.launch_count()
-    frame_ms = timed_frames(torch, native, r, vp, sp, stream, outs, flush)
-    launches = native.launch_count() - launches0
-    cache.join(sp)
-    t_end.record(stream)
-    torch.cuda.synchronize()
-    cache_ms = [t_start.elapsed_time(t_end) / steps] * steps
+    cmp = cache_comparison(torch, native, w, dev, steps, args.warmup, args.train_samples, [args.train_suffix],
+                           args.seed)
     if world > 1:
         dist.barrier()
     clock_info = clocks.stop()
-    stats = {s["name"]: s for s in native.stage_stats()}
-    cstats = cache.stats()
-
-    # per-frame quality against the plain depth-8 frame
-    ref_pix = ref[0][0]
-    ref8 = torch.floor(255.0 * torch.sqrt(ref_pix[:, :3].clamp(0, 1)))
-    psnr, max_abs = [], []
-    for pix, _ in outs:
-        p8 = torch.floor(255.0 * torch.sqrt(pix[:, :3].clamp(0, 1)))
-        mse = float(((p8 - ref8) ** 2).mean())
-        psnr.append(99.0 if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse))
-        max_abs.append(float((pix[:, :3] - ref_pix[:, :3]).abs().max()))
-    cache_rays = counted(L.CACHE_ON)
+    c = cmp["cache"][0]
 
     # end to end through the C ABI with host buffers, cache on
+    r = RayTracingRenderer(w.scene, 8)
+    RadianceCache.configure(cache_depth=2, train_samples=args.train_samples, batch=16384, seed=args.seed,
+                            train_suffix=args.train_suffix)
     native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
     pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
@@ -484,7 +559,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     cv, _, _ = make_canvas(w.width, w.height, L.AA_NONE)
     cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
     proj = w.projection()
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, CACHE_WARMUP_FRAMES)):
         native.check(lib.slimUploadGeometries(native.ptr(sd)))
         native.check(lib.slimRefitSceneBVH(None))
         native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
@@ -496,46 +571,28 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     e2e_s = time.perf_counter() - t0
     native.set_render_options(engine=L.ENGINE_WAVEFRONT)
 
-    cache_total, plain_total, e2e_s = max_over_ranks([sum(cache_ms), sum(plain_ms), e2e_s], dev, world)
-    value = whole_job_rate(cache_rays, steps, world, cache_total)
-    timed = {k: v for k, v in stats.items() if v["launches"]}
-    stages = {k: v["total_ms"] / steps for k, v in timed.items()}
-    q = stats.get("cache_query")
-    nrc_roofline = None
-    if q and q["launches"]:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-        peak_tf = float(peaks.get("bf16_tflops", 1590.0))
-        ach = cstats["queries"] * NRC_FLOPS_PER_QUERY / (q["total_ms"] / q["launches"] / 1000.0) / 1e12
-        nrc_roofline = {"kernel": "k_nrc_infer", "bound": "tensor", "achieved": ach, "peak": peak_tf,
-                        "unit": "TFLOP/s", "frac": ach / peak_tf, "flops_per_query": NRC_FLOPS_PER_QUERY,
-                        "queries": cstats["queries"], "ms_per_launch": q["total_ms"] / q["launches"],
-                        "peak_source": "measured (MEASURED_PEAKS.json bf16_tflops)" if peaks else "fallback"}
-    dom = max(timed, key=lambda k: timed[k]["total_ms"]) if timed else None
+    cache_total, plain_total, e2e_s = max_over_ranks([c["ms_per_frame"] * steps,
+                                                      cmp["plain_depth8"]["ms_per_frame"] * steps, e2e_s], dev, world)
+    value = whole_job_rate(c["rays_per_frame"], steps, world, cache_total)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": cache_total / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded config2 scene, depth 8)",
             "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 8, "cache_depth": 2,
-                       "train_samples_per_frame": args.train_samples, "batch": 16384, "learning_rate": 1e-2,
-                       "cache_warmup_frames": cache_warmup,
+                       "train_samples_per_frame": args.train_samples, "train_suffix": args.train_suffix,
+                       "batch": 16384, "learning_rate": 1e-2, "cache_warmup_frames": c["cache_warmup_frames"],
                        "engine": "wavefront", "parallelism": f"replicas x{world}",
-                       "l2": "flushed between steps (512 MiB write)", "rays_per_frame": cache_rays},
+                       "l2": "flushed between steps (512 MiB write)", "rays_per_frame": c["rays_per_frame"]},
             "ms_per_frame": cache_total / steps,
-            "plain_depth8": {"ms_per_frame": plain_total / steps, "rays_per_frame": plain_rays,
-                             "mrays_s": plain_rays * steps * world / (plain_total / 1000.0) / 1e6,
-                             "stages_ms_per_frame": plain_stages},
+            "plain_depth8": cmp["plain_depth8"],
             "speedup_vs_plain_depth8": plain_total / cache_total,
-            "psnr_db_per_frame": psnr, "max_abs_per_frame": max_abs,
-            "frame_event_ms": frame_ms,
-            "cache": {"queries": cstats["queries"], "train_samples": cstats["train_samples"],
-                      "loss": cstats["loss"], "steps": cstats["steps"], "frames": cstats["frames"]},
-            "stages_ms_per_frame": stages, "dominant_stage": dom,
-            "roofline": nrc_roofline,
-            "e2e": {"value": cache_rays * steps * world / e2e_s / 1e6, "unit": UNIT,
+            "psnr_db_per_frame": c["psnr_db_per_frame"], "max_abs_per_frame": c["max_abs_per_frame"],
+            "cache": {k: c[k] for k in ("queries", "train_samples", "loss", "train_targets")},
+            "e2e": {"value": c["rays_per_frame"] * steps * world / e2e_s / 1e6, "unit": UNIT,
                     "h2d_bytes_per_step": int(w.scene.geometries.nbytes),
                     "d2h_bytes_per_step": int(pin_pix.numel() * 4 + pin_dep.numel() * 4),
                     "ms_per_step": 1000.0 * e2e_s / steps},
             "clocks": clock_info,
-            "gpu_launches": launches}
+            "gpu_launches": c["gpu_launches"]}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -825,6 +882,15 @@ def main():
                     "ms_per_step": 1000.0 * e2e_s / args.steps},
             "clocks": clock_info,
             "gpu_launches": launches}
+    if args.config == "config2" and args.engine == "wavefront" and not args.no_cache_block:
+        # the metric's second half, in the same process: config 4 (this scene at
+        # bounce depth 8), plain frames against radiance-cache frames
+        w4 = scenes.config4(args.seed, meshes=w.scene.meshes)
+        cmp = cache_comparison(torch, native, w4, dev, min(args.steps, 10), args.warmup, args.train_samples, [0, 1],
+                               args.seed)
+        cmp["workload"] = w4.name
+        cmp["nrc_roofline"] = nrc_roofline(torch, native, w4, dev)
+        line["radiance_cache"] = cmp
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(w, args.cpu_seconds).items() if k != "seconds"}
     if rank == 0:

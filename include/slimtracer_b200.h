@@ -394,7 +394,13 @@ typedef struct {
                                 on a second stream, one frame behind: a frame's queries are
                                 answered with the weights trained through the previous frame,
                                 while its own training overlaps the next frame's rays */
-    uint32_t _reserved[2];
+    uint32_t train_suffix;   /* 0: every training path is traced to max_depth (its target is
+                                the tracer's full-depth radiance).  k > 0: a training path is
+                                traced k bounces past the cache vertex and, where it is still
+                                going there, ends in the cache's own answer for that vertex
+                                (self-training: targets cost k rounds instead of
+                                max_depth - cache_depth + 1); max_depth still ends paths */
+    uint32_t _reserved;
 } SlimRadianceCacheConfig;
 typedef struct {
     uint64_t frames, steps;  /* frames rendered with the cache, Adam steps taken */
@@ -510,6 +516,51 @@ int slimReadTextureHeader(const char *path, SlimTexture *texture, uint32_t *tota
 int slimReadTexture(const char *path, SlimTexture *texture, SlimTextureMip *mips,
                     SlimTexelQuad *texel_quads);
 int slimWriteTexture(const char *path, const SlimTexture *texture);
+
+/* Whole-scene files: save/load(Scene&, SceneIO&) (serialization/scene.h:5-109).
+ * A scene file holds SlimSceneCounts (44 bytes); every mesh's .mesh header
+ * (7 u32: vertex, triangle, edge, uv and normal counts, BVH node count and
+ * height); every texture's ImageInfo (32 bytes); per camera focal_length,
+ * zoom_amount, dolly_amount, target_distance (f32 each), current_velocity,
+ * position (vec3) and the orientation (48 bytes); the geometries (72 bytes
+ * each); the viewport overlay's grids, boxes and curves (records of
+ * SLIM_GRID_BYTES, SLIM_BOX_BYTES and SLIM_CURVE_BYTES, kept opaque here);
+ * then every mesh's content (a .mesh file after its header) and every
+ * texture's mips (a .texture file after its ImageInfo).  Lights and
+ * materials are not in the file, as in the reference. */
+typedef struct {                                              /* scene/camera.h:6-13 */
+    float orientation[9];    /* OrientationUsing3x3Matrix: columns X (right), Y (up), Z (forward) */
+    float rotation[3];       /* its x, y, z angles (radians) */
+    SlimVec3 position, current_velocity;
+    float focal_length, zoom_amount, target_distance, dolly_amount;
+} SlimCamera;
+#define SLIM_GRID_BYTES  9700   /* sizeof(Grid),  scene/grid.h  */
+#define SLIM_BOX_BYTES    384   /* sizeof(Box),   scene/box.h   */
+#define SLIM_CURVE_BYTES   12   /* sizeof(Curve), core/base.h   */
+typedef struct {
+    SlimSceneCounts counts;  /* of the arrays below (lights, materials, tets, quads: not in the file) */
+    uint32_t _pad;
+    SlimCamera *cameras;
+    SlimGeometry *geometries;
+    SlimMesh *meshes;        /* records whose arrays the caller allocates */
+    SlimTexture *textures;   /* records with caller-allocated mips and texel quads */
+    void *grids, *boxes, *curves;
+} SlimSceneFile;
+SLIM_STATIC_ASSERT(sizeof(SlimCamera) == 88, "Camera is 88 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimSceneFile) == 104, "SceneFile is 104 bytes");
+
+int slimSaveScene(const char *path, const SlimSceneFile *scene);
+/* Sizing pass of a load.  Fills scene->counts; when scene->meshes and
+ * scene->textures are given (records for counts.meshes / counts.textures),
+ * also every mesh's counts (vertex ... normals counts, bvh.node_count,
+ * bvh.height) and every texture's ImageInfo fields and mip_count, and, when
+ * texel_quad_counts is given, the texel quads of each texture's mips. */
+int slimReadSceneHeader(const char *path, SlimSceneFile *scene, uint32_t *texel_quad_counts);
+/* Reads the whole file into the caller's arrays: cameras, geometries,
+ * grids, boxes, curves, and every mesh's and texture's arrays (texture
+ * mips point into one texel-quad array per texture, as slimReadTexture
+ * sets them).  The counts must equal the file's. */
+int slimLoadScene(const char *path, SlimSceneFile *scene);
 
 /* bmp2texture's texel-quad baker (bmp2texture.cpp:24-237,255-335) from
  * 8-bit BGR(A) rows as a BMP stores them after its own flip handling.

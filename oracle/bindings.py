@@ -287,3 +287,68 @@ def reference_build_mesh(positions, indices, normals=None, normal_indices=None, 
                                     _ptr(nodes), _ptr(nc), _ptr(ht), _ptr(aabb), _ptr(out_pos))
     assert rc == 0
     return tris, nodes[:int(nc[0])], int(ht[0]), aabb, out_pos
+
+
+def reference_scene_record_sizes():
+    """sizeof Camera, OrientationUsing3x3Matrix, Grid, Box, Curve,
+    SceneCounts, ImageInfo, Geometry in the reference build."""
+    h = reference()
+    out = np.zeros(8, np.uint32)
+    h.ref_scene_record_sizes.argtypes = [P]
+    h.ref_scene_record_sizes(_ptr(out))
+    return [int(x) for x in out]
+
+
+def _reference_scene_data(scene_file_record, layout):
+    """A reference SceneData pointing at the arrays of a SlimSceneFile record
+    (the members save/load read: counts, cameras, geometries, meshes,
+    textures, grids, boxes, curves)."""
+    sd = np.zeros((), layout.SCENE_DATA)
+    sd["counts"] = scene_file_record["counts"]
+    for k in ("cameras", "geometries", "meshes", "textures", "grids", "boxes", "curves"):
+        sd[k] = scene_file_record[k]
+    return sd
+
+
+def reference_save_scene(scene_file, path, layout):
+    """The reference's save(Scene&, SceneIO&) on a SceneFile's arrays."""
+    h = reference()
+    h.ref_save_scene.argtypes = [P, C.c_char_p]
+    rec = scene_file.record()
+    sd = _reference_scene_data(rec, layout)
+    rc = h.ref_save_scene(_ptr(sd), str(path).encode())
+    assert rc == 0
+
+
+def reference_load_scene(path, like, layout):
+    """The reference's load(Scene&, SceneIO&) into fresh arrays shaped like
+    the SceneFile `like` (its counts, mesh counts and mip sizes), returned
+    as a SceneFile.  The reference sizes these arrays from the mesh and
+    texture files its app loads before the scene file."""
+    import copy
+    from slimtracincpp_b200.scene import MeshAsset, TextureAsset
+    from slimtracincpp_b200.scene_file import SceneFile
+    meshes = []
+    for m in like.meshes:
+        z = lambda a: None if a is None else np.zeros_like(a)
+        meshes.append(MeshAsset(np.zeros_like(m.triangles), np.zeros_like(m.nodes), np.zeros(3), np.zeros(3), 0,
+                                np.zeros_like(m.positions), np.zeros_like(m.position_indices), z(m.normals),
+                                z(m.normal_indices), z(m.uvs), z(m.uv_indices), np.zeros_like(m.edges)))
+    textures = [TextureAsset(np.zeros((), layout.TEXTURE), t.mip_sizes, np.zeros_like(t.quads)) for t in like.textures]
+    out = SceneFile(np.zeros_like(like.geometries), meshes, textures, np.zeros_like(like.cameras),
+                    np.zeros_like(like.grids), np.zeros_like(like.boxes), np.zeros_like(like.curves))
+    rec = out.record()
+    sd = _reference_scene_data(rec, layout)
+    h = reference()
+    h.ref_load_scene.argtypes = [P, C.c_char_p]
+    rc = h.ref_load_scene(_ptr(sd), str(path).encode())
+    assert rc == 0
+    # the reference wrote the headers into the records: carry them back
+    for i, m in enumerate(out.meshes):
+        r = out._mesh_records[i]
+        m.aabb_min, m.aabb_max, m.height = r["aabb_min"].copy(), r["aabb_max"].copy(), int(r["bvh_height"])
+    for i, t in enumerate(out.textures):
+        r = out._texture_records[i]
+        for k in ("width", "height", "size", "stride", "tile_width", "tile_height", "mip_count", "flags"):
+            t.header[k] = r[k]
+    return out

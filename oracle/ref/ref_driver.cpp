@@ -21,6 +21,8 @@
  *                         (renderer/renderer.h:87-100)
  *   ref_trace_primary     SceneTracer::trace of each primary ray
  *                         (renderer/ray_tracer.h:36-45, scene/scene_tracer.h:26-98)
+ *   ref_save_scene / ref_load_scene   save/load(Scene&, SceneIO&)
+ *                         (serialization/scene.h:5-109), ref_scene_record_sizes
  */
 #include <atomic>
 #include <cstdio>
@@ -33,6 +35,7 @@
 
 #include "slim/math/vec2.h"
 #include "slim/renderer/renderer.h"
+#include "slim/serialization/scene.h"
 
 static_assert(sizeof(u32) == 4, "reference u32 must be 4 bytes");
 static_assert(sizeof(Geometry) == 72, "Geometry layout");
@@ -354,6 +357,36 @@ int ref_trace_primary(const void *scene_data, const void *projection_data, int w
             }
         free(ctx);
     });
+    return 0;
+}
+
+// Sizes of the records a scene file holds (serialization/scene.h:5-109):
+// Camera, its OrientationUsing3x3Matrix, Grid, Box, Curve, SceneCounts,
+// ImageInfo, Geometry.
+int ref_scene_record_sizes(unsigned *out) {
+    out[0] = sizeof(Camera); out[1] = sizeof(OrientationUsing3x3Matrix); out[2] = sizeof(Grid);
+    out[3] = sizeof(Box); out[4] = sizeof(Curve); out[5] = sizeof(SceneCountsData); out[6] = sizeof(ImageInfo);
+    out[7] = sizeof(Geometry);
+    return 0;
+}
+
+// save(Scene&, SceneIO&) (serialization/scene.h:59-109) on a caller-owned
+// SceneData (counts, cameras, geometries, grids, boxes, curves, meshes,
+// textures are the members it reads).
+int ref_save_scene(void *scene_data, const char *path) {
+    SceneIO io;
+    io.file_path = String(path);
+    save(*(Scene*)scene_data, io);
+    return 0;
+}
+
+// load(Scene&, SceneIO&) (serialization/scene.h:5-57) into caller-allocated
+// arrays sized from the file (the reference's own app sizes them from the
+// mesh and texture files it loads first).
+int ref_load_scene(void *scene_data, const char *path) {
+    SceneIO io;
+    io.file_path = String(path);
+    load(*(Scene*)scene_data, io);
     return 0;
 }
 

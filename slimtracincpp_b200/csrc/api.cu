@@ -203,6 +203,8 @@ struct Context {
         DevArray<float> params, m, v, grad, partials, loss_partials, loss;
         DevArray<uint8_t> image;
         DevArray<float4> features, aux, radiance, t_features, t_targets, t_color, t_through;
+        DevArray<float4> s_features, s_aux, s_radiance;   // self-training queries
+        DevArray<uint32_t> s_count;
         DevArray<uint32_t> counts;
         DevArray<uint32_t> state;      // [0] Adam steps taken, [1] cache frames (training-set offsets)
         uint32_t *error_flags = nullptr;
@@ -645,6 +647,12 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
         if ((rc = k.t_color.reserve(cap, "alloc training paths"))) return rc;
         if ((rc = k.t_through.reserve(cap, "alloc training paths"))) return rc;
         if (mode == SLIM_CACHE_ON && (rc = k.t_features.reserve(4 * (size_t)cap, "alloc training samples"))) return rc;
+        if (mode == SLIM_CACHE_ON && k.config.train_suffix) {
+            if ((rc = k.s_features.reserve(4 * (size_t)cap, "alloc self-training queries"))) return rc;
+            if ((rc = k.s_aux.reserve(2 * (size_t)cap, "alloc self-training queries"))) return rc;
+            if ((rc = k.s_radiance.reserve(cap, "alloc self-training answers"))) return rc;
+            if ((rc = k.s_count.reserve(1, "alloc self-training counter"))) return rc;
+        }
     }
     cf.mode = mode;
     cf.depth = k.config.cache_depth;
@@ -661,6 +669,13 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     cf.batch = k.config.batch;
     cf.weights = k.image.ptr;
     cf.trainer = (mode == SLIM_CACHE_ON && k.config.train) ? &k : nullptr;
+    if (mode == SLIM_CACHE_ON && k.config.train_suffix && cap) {
+        cf.train_suffix = k.config.train_suffix;
+        cf.s_features = k.s_features.ptr;
+        cf.s_aux = k.s_aux.ptr;
+        cf.s_radiance = k.s_radiance.ptr;
+        cf.s_count = k.s_count.ptr;
+    }
     k.error_flags = c.d_error.ptr;
     // Overlapped training (not while counting work: the counters of a frame
     // must be complete when the frame's stream is).
@@ -1338,6 +1353,11 @@ int slimReadTexture(const char *path, SlimTexture *texture, SlimTextureMip *mips
     return slim::read_texture(path, texture, mips, texel_quads);
 }
 int slimWriteTexture(const char *path, const SlimTexture *texture) { return slim::write_texture(path, texture); }
+int slimSaveScene(const char *path, const SlimSceneFile *scene) { return slim::save_scene(path, scene); }
+int slimReadSceneHeader(const char *path, SlimSceneFile *scene, uint32_t *texel_quad_counts) {
+    return slim::read_scene_header(path, scene, texel_quad_counts);
+}
+int slimLoadScene(const char *path, SlimSceneFile *scene) { return slim::load_scene(path, scene); }
 int slimBakeTexture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
                     SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *texel_quads, uint32_t *mip_count,
                     uint32_t *texel_quad_count) {
@@ -1546,7 +1566,7 @@ int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
     const SlimRadianceCacheConfig &k = *config;
     if (k.cache_depth < 2 || k.cache_depth > 255 || !k.batch || !(k.learning_rate > 0.0f) || !(k.beta1 >= 0.0f) ||
         !(k.beta1 < 1.0f) || !(k.beta2 >= 0.0f) || !(k.beta2 < 1.0f) || !(k.epsilon > 0.0f) ||
-        k.train_samples > (1u << 26))
+        k.train_samples > (1u << 26) || k.train_suffix > 255)
         return set_error(SLIM_ERR_ARGUMENT, "bad radiance cache config");
     Context::Cache &st = c.cache;
     invalidate_batch();

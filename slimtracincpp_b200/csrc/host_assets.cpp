@@ -565,4 +565,244 @@ int write_texture(const char *path, const SlimTexture *t) {
     return ok ? SLIM_OK : set_error(SLIM_ERR_IO, "slimWriteTexture: write failed");
 }
 
+// ---- whole-scene files (serialization/scene.h:5-109) ------------------------
+// Sections in file order: counts; mesh headers; texture ImageInfos; cameras;
+// geometries; grids, boxes, curves; mesh contents; texture mips.
+namespace {
+
+constexpr size_t kCameraFileBytes = 4 * 4 + 12 + 12 + 48;   // the fields save() writes per camera
+
+bool write_mesh_header(File &f, const SlimMesh &m) {
+    uint32_t h[7] = {m.vertex_count, m.triangle_count, m.edge_count, m.uvs_count, m.normals_count, m.bvh.node_count,
+                     m.bvh.height};
+    return f.write(h, sizeof(h));
+}
+
+bool write_mesh_content(File &f, const SlimMesh &m) {
+    bool ok = f.write(&m.aabb, sizeof(SlimAABB)) &&
+              f.write(m.triangles, sizeof(SlimTriangle) * (size_t)m.triangle_count) &&
+              f.write(m.vertex_positions, sizeof(SlimVec3) * (size_t)m.vertex_count) &&
+              f.write(m.vertex_position_indices, 12 * (size_t)m.triangle_count) &&
+              f.write(m.edge_vertex_indices, 8 * (size_t)m.edge_count);
+    if (ok && m.uvs_count)
+        ok = f.write(m.vertex_uvs, sizeof(SlimVec2) * (size_t)m.uvs_count) &&
+             f.write(m.vertex_uvs_indices, 12 * (size_t)m.triangle_count);
+    if (ok && m.normals_count)
+        ok = f.write(m.vertex_normals, sizeof(SlimVec3) * (size_t)m.normals_count) &&
+             f.write(m.vertex_normal_indices, 12 * (size_t)m.triangle_count);
+    return ok && f.write(m.bvh.nodes, sizeof(SlimBVHNode) * (size_t)m.bvh.node_count);
+}
+
+bool read_mesh_content(File &f, SlimMesh &m) {
+    bool ok = f.read(&m.aabb, sizeof(SlimAABB)) &&
+              f.read(m.triangles, sizeof(SlimTriangle) * (size_t)m.triangle_count) &&
+              f.read(m.vertex_positions, sizeof(SlimVec3) * (size_t)m.vertex_count) &&
+              f.read(m.vertex_position_indices, 12 * (size_t)m.triangle_count) &&
+              f.read(m.edge_vertex_indices, 8 * (size_t)m.edge_count);
+    if (ok && m.uvs_count)
+        ok = f.read(m.vertex_uvs, sizeof(SlimVec2) * (size_t)m.uvs_count) &&
+             f.read(m.vertex_uvs_indices, 12 * (size_t)m.triangle_count);
+    if (ok && m.normals_count)
+        ok = f.read(m.vertex_normals, sizeof(SlimVec3) * (size_t)m.normals_count) &&
+             f.read(m.vertex_normal_indices, 12 * (size_t)m.triangle_count);
+    return ok && f.read(m.bvh.nodes, sizeof(SlimBVHNode) * (size_t)m.bvh.node_count);
+}
+
+size_t mesh_content_bytes(const SlimMesh &m) {
+    size_t t = m.triangle_count;
+    size_t b = sizeof(SlimAABB) + sizeof(SlimTriangle) * t + sizeof(SlimVec3) * (size_t)m.vertex_count + 12 * t +
+               8 * (size_t)m.edge_count;
+    if (m.uvs_count) b += sizeof(SlimVec2) * (size_t)m.uvs_count + 12 * t;
+    if (m.normals_count) b += sizeof(SlimVec3) * (size_t)m.normals_count + 12 * t;
+    return b + sizeof(SlimBVHNode) * (size_t)m.bvh.node_count;
+}
+
+bool write_camera(File &f, const SlimCamera &c) {
+    float orientation[12];
+    memcpy(orientation, c.orientation, 36);
+    memcpy(orientation + 9, c.rotation, 12);
+    return f.write(&c.focal_length, 4) && f.write(&c.zoom_amount, 4) && f.write(&c.dolly_amount, 4) &&
+           f.write(&c.target_distance, 4) && f.write(&c.current_velocity, 12) && f.write(&c.position, 12) &&
+           f.write(orientation, 48);
+}
+
+bool read_camera(File &f, SlimCamera &c) {
+    float orientation[12];
+    bool ok = f.read(&c.focal_length, 4) && f.read(&c.zoom_amount, 4) && f.read(&c.dolly_amount, 4) &&
+              f.read(&c.target_distance, 4) && f.read(&c.current_velocity, 12) && f.read(&c.position, 12) &&
+              f.read(orientation, 48);
+    if (ok) {
+        memcpy(c.orientation, orientation, 36);
+        memcpy(c.rotation, orientation + 9, 12);
+    }
+    return ok;
+}
+
+bool check_counts(uint32_t n, const void *p) { return n == 0 || p != nullptr; }
+
+// The counts a scene file's readers use, from its first 44 bytes.
+bool read_counts(File &f, SlimSceneCounts &counts) {
+    if (!f.read(&counts, sizeof(SlimSceneCounts))) return false;
+    const uint32_t limit = 1u << 24;
+    return counts.geometries < limit && counts.cameras < limit && counts.textures < 256 && counts.meshes < limit &&
+           counts.grids < limit && counts.boxes < limit && counts.curves < limit;
+}
+
+bool skip(File &f, size_t bytes) { return bytes == 0 || fseek(f.f, (long)bytes, SEEK_CUR) == 0; }
+
+}  // namespace
+
+int save_scene(const char *path, const SlimSceneFile *sc) {
+    if (!path || !sc) return set_error(SLIM_ERR_ARGUMENT, "slimSaveScene: null argument");
+    const SlimSceneCounts &n = sc->counts;
+    if (!check_counts(n.cameras, sc->cameras) || !check_counts(n.geometries, sc->geometries) ||
+        !check_counts(n.meshes, sc->meshes) || !check_counts(n.textures, sc->textures) ||
+        !check_counts(n.grids, sc->grids) || !check_counts(n.boxes, sc->boxes) || !check_counts(n.curves, sc->curves))
+        return set_error(SLIM_ERR_ARGUMENT, "slimSaveScene: an array with a non-zero count is null");
+    for (uint32_t i = 0; i < n.meshes; i++) {
+        const SlimMesh &m = sc->meshes[i];
+        if (!m.triangles || !m.vertex_positions || !m.vertex_position_indices || !m.bvh.nodes ||
+            (m.edge_count && !m.edge_vertex_indices) || (m.uvs_count && (!m.vertex_uvs || !m.vertex_uvs_indices)) ||
+            (m.normals_count && (!m.vertex_normals || !m.vertex_normal_indices)))
+            return set_error(SLIM_ERR_ARGUMENT, "slimSaveScene: mesh arrays missing");
+    }
+    for (uint32_t i = 0; i < n.textures; i++)
+        if (!sc->textures[i].mips || !sc->textures[i].mip_count)
+            return set_error(SLIM_ERR_ARGUMENT, "slimSaveScene: texture without mips");
+    File f(path, "wb");
+    if (!f.f) return set_error(SLIM_ERR_IO, "slimSaveScene: cannot open file");
+    bool ok = f.write(&n, sizeof(SlimSceneCounts));
+    for (uint32_t i = 0; ok && i < n.meshes; i++) ok = write_mesh_header(f, sc->meshes[i]);
+    for (uint32_t i = 0; ok && i < n.textures; i++) ok = f.write(&sc->textures[i], 32);
+    for (uint32_t i = 0; ok && i < n.cameras; i++) ok = write_camera(f, sc->cameras[i]);
+    ok = ok && f.write(sc->geometries, sizeof(SlimGeometry) * (size_t)n.geometries) &&
+         f.write(sc->grids, (size_t)SLIM_GRID_BYTES * n.grids) && f.write(sc->boxes, (size_t)SLIM_BOX_BYTES * n.boxes) &&
+         f.write(sc->curves, (size_t)SLIM_CURVE_BYTES * n.curves);
+    for (uint32_t i = 0; ok && i < n.meshes; i++) ok = write_mesh_content(f, sc->meshes[i]);
+    for (uint32_t i = 0; ok && i < n.textures; i++) {
+        const SlimTexture &t = sc->textures[i];
+        for (uint32_t m = 0; ok && m < t.mip_count; m++) {
+            const SlimTextureMip &mip = t.mips[m];
+            ok = f.write(&mip.width, 4) && f.write(&mip.height, 4) &&
+                 f.write(mip.texel_quads, sizeof(SlimTexelQuad) * (size_t)(mip.width + 1) * (size_t)(mip.height + 1));
+        }
+    }
+    return ok ? SLIM_OK : set_error(SLIM_ERR_IO, "slimSaveScene: write failed");
+}
+
+int read_scene_header(const char *path, SlimSceneFile *sc, uint32_t *texel_quad_counts) {
+    if (!path || !sc) return set_error(SLIM_ERR_ARGUMENT, "slimReadSceneHeader: null argument");
+    File f(path, "rb");
+    if (!f.f) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: cannot open file");
+    if (!read_counts(f, sc->counts)) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated or bad counts");
+    const SlimSceneCounts n = sc->counts;
+    if ((n.meshes && !sc->meshes) || (n.textures && !sc->textures)) return SLIM_OK;   // counts only
+    for (uint32_t i = 0; i < n.meshes; i++) {
+        uint32_t h[7];
+        if (!f.read(h, sizeof(h))) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated mesh header");
+        SlimMesh &m = sc->meshes[i];
+        m.vertex_count = h[0]; m.triangle_count = h[1]; m.edge_count = h[2];
+        m.uvs_count = h[3]; m.normals_count = h[4];
+        m.bvh.node_count = h[5]; m.bvh.height = (uint8_t)(h[6] & 0xFF);
+        if (!m.triangle_count || !m.vertex_count || !m.bvh.node_count || m.bvh.node_count > 2 * m.triangle_count)
+            return set_error(SLIM_ERR_IO, "slimReadSceneHeader: malformed mesh counts");
+    }
+    for (uint32_t i = 0; i < n.textures; i++) {
+        SlimTexture &t = sc->textures[i];
+        SlimTextureMip *mips = t.mips;
+        if (!f.read(&t, 32)) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated texture header");
+        t.mips = mips;
+        if (!t.mip_count || t.mip_count > 16) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: bad mip count");
+    }
+    if (!texel_quad_counts) return SLIM_OK;
+    size_t fixed = kCameraFileBytes * n.cameras + sizeof(SlimGeometry) * (size_t)n.geometries +
+                   (size_t)SLIM_GRID_BYTES * n.grids + (size_t)SLIM_BOX_BYTES * n.boxes + (size_t)SLIM_CURVE_BYTES * n.curves;
+    for (uint32_t i = 0; i < n.meshes; i++) fixed += mesh_content_bytes(sc->meshes[i]);
+    if (!skip(f, fixed)) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated");
+    for (uint32_t i = 0; i < n.textures; i++) {
+        uint64_t total = 0;
+        for (uint32_t m = 0; m < sc->textures[i].mip_count; m++) {
+            uint32_t wh[2];
+            if (!f.read(wh, 8)) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated texture");
+            uint64_t q = (uint64_t)(wh[0] + 1ull) * (uint64_t)(wh[1] + 1ull);
+            if (!wh[0] || !wh[1] || q > (1ull << 31)) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: bad mip size");
+            total += q;
+            if (!skip(f, q * sizeof(SlimTexelQuad))) return set_error(SLIM_ERR_IO, "slimReadSceneHeader: truncated");
+        }
+        if (total > 0xFFFFFFFFull) return set_error(SLIM_ERR_LIMIT, "slimReadSceneHeader: too many texel quads");
+        texel_quad_counts[i] = (uint32_t)total;
+    }
+    return SLIM_OK;
+}
+
+int load_scene(const char *path, SlimSceneFile *sc) {
+    if (!path || !sc) return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: null argument");
+    File f(path, "rb");
+    if (!f.f) return set_error(SLIM_ERR_IO, "slimLoadScene: cannot open file");
+    SlimSceneCounts n;
+    if (!read_counts(f, n)) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated or bad counts");
+    const SlimSceneCounts &c = sc->counts;
+    if (n.geometries != c.geometries || n.cameras != c.cameras || n.textures != c.textures || n.meshes != c.meshes ||
+        n.grids != c.grids || n.boxes != c.boxes || n.curves != c.curves)
+        return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: counts differ from the file's");
+    if (!check_counts(n.cameras, sc->cameras) || !check_counts(n.geometries, sc->geometries) ||
+        !check_counts(n.meshes, sc->meshes) || !check_counts(n.textures, sc->textures) ||
+        !check_counts(n.grids, sc->grids) || !check_counts(n.boxes, sc->boxes) || !check_counts(n.curves, sc->curves))
+        return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: an array with a non-zero count is null");
+    for (uint32_t i = 0; i < n.meshes; i++) {
+        uint32_t h[7];
+        if (!f.read(h, sizeof(h))) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated mesh header");
+        const SlimMesh &m = sc->meshes[i];
+        if (h[0] != m.vertex_count || h[1] != m.triangle_count || h[2] != m.edge_count || h[3] != m.uvs_count ||
+            h[4] != m.normals_count || h[5] != m.bvh.node_count)
+            return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: mesh counts differ from the file's");
+        if (!m.triangles || !m.vertex_positions || !m.vertex_position_indices || !m.bvh.nodes ||
+            (m.edge_count && !m.edge_vertex_indices) || (m.uvs_count && (!m.vertex_uvs || !m.vertex_uvs_indices)) ||
+            (m.normals_count && (!m.vertex_normals || !m.vertex_normal_indices)))
+            return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: mesh arrays missing");
+    }
+    std::vector<SlimTexelQuad *> quads(n.textures, nullptr);
+    for (uint32_t i = 0; i < n.textures; i++) {
+        SlimTexture &t = sc->textures[i];
+        SlimTextureMip *mips = t.mips;
+        if (!mips || !mips[0].texel_quads) return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: texture buffers missing");
+        quads[i] = mips[0].texel_quads;
+        uint32_t mip_count = t.mip_count;
+        if (!f.read(&t, 32)) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated texture header");
+        t.mips = mips;
+        if (t.mip_count != mip_count) return set_error(SLIM_ERR_ARGUMENT, "slimLoadScene: mip count differs from the file's");
+    }
+    bool ok = true;
+    for (uint32_t i = 0; ok && i < n.cameras; i++) ok = read_camera(f, sc->cameras[i]);
+    ok = ok && f.read(sc->geometries, sizeof(SlimGeometry) * (size_t)n.geometries) &&
+         f.read(sc->grids, (size_t)SLIM_GRID_BYTES * n.grids) && f.read(sc->boxes, (size_t)SLIM_BOX_BYTES * n.boxes) &&
+         f.read(sc->curves, (size_t)SLIM_CURVE_BYTES * n.curves);
+    for (uint32_t i = 0; ok && i < n.meshes; i++) ok = read_mesh_content(f, sc->meshes[i]);
+    if (!ok) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated file");
+    for (uint32_t i = 0; i < n.meshes; i++) {
+        const SlimMesh &m = sc->meshes[i];
+        for (uint32_t k = 0; k < m.bvh.node_count; k++) {
+            const SlimBVHNode &b = m.bvh.nodes[k];
+            if (b.leaf_count ? (uint64_t)b.first_index + b.leaf_count > m.triangle_count
+                             : (uint64_t)b.first_index + 1 >= m.bvh.node_count)
+                return set_error(SLIM_ERR_IO, "slimLoadScene: BVH node index out of range");
+        }
+    }
+    for (uint32_t i = 0; i < n.textures; i++) {
+        SlimTexture &t = sc->textures[i];
+        SlimTexelQuad *q = quads[i];
+        for (uint32_t m = 0; m < t.mip_count; m++) {
+            uint32_t wh[2];
+            if (!f.read(wh, 8)) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated texture");
+            size_t count = (size_t)(wh[0] + 1) * (size_t)(wh[1] + 1);
+            if (!f.read(q, count * sizeof(SlimTexelQuad))) return set_error(SLIM_ERR_IO, "slimLoadScene: truncated texture");
+            t.mips[m].width = wh[0];
+            t.mips[m].height = wh[1];
+            t.mips[m].texel_quads = q;
+            q += count;
+        }
+    }
+    return SLIM_OK;
+}
+
 }  // namespace slim

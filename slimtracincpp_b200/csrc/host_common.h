@@ -24,6 +24,9 @@ int write_mesh(const char *path, const SlimMesh *m);
 int read_texture_header(const char *path, SlimTexture *t, uint32_t *total_quads);
 int read_texture(const char *path, SlimTexture *t, SlimTextureMip *mips, SlimTexelQuad *quads);
 int write_texture(const char *path, const SlimTexture *t);
+int save_scene(const char *path, const SlimSceneFile *scene);
+int read_scene_header(const char *path, SlimSceneFile *scene, uint32_t *texel_quad_counts);
+int load_scene(const char *path, SlimSceneFile *scene);
 int bake_texture(const uint8_t *bgr, uint32_t width, uint32_t height, uint32_t channels, uint32_t flags,
                  SlimTexture *texture, SlimTextureMip *mips, SlimTexelQuad *quads, uint32_t *mip_count,
                  uint32_t *quad_count);

@@ -88,6 +88,12 @@ struct CacheFrame {
     const WavefrontBuffers *train_queues = nullptr;
     const uint8_t *train_weights = nullptr;   // image the training updates; copied into `weights`
                                               // (what the queries read) once per frame
+    // Self-training (train_suffix > 0): the training paths stop train_suffix
+    // bounces past the cache vertex and query the cache there; those queries
+    // go to their own buffers (one slot per training path).
+    uint32_t train_suffix = 0;
+    float4 *s_features = nullptr, *s_aux = nullptr, *s_radiance = nullptr;
+    uint32_t *s_count = nullptr;
 };
 
 // Download of a frame's (or band's) canvas rows while its later bounces

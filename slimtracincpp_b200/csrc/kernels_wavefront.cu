@@ -1147,6 +1147,7 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
     add_glow(S, ray, hit_distance, current);
     color = mul_add(current, throughput, color);
     if (query) A.path_color[path] = make_float4(color.x, color.y, color.z, pc.w);
+    else if (A.sink) A.sink[path] = make_float4(color.x, color.y, color.z, 0.0f);   // a self-training path ends
     else write_pixel<BATCH>(F, pid, color, pc.w);
     return query;
 }
@@ -1314,6 +1315,20 @@ __global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *C.train_count = n;
         *ray_count = n;
+    }
+}
+
+// Self-training targets: a training path that reached its cache vertex
+// (query q of the self-training set) ends in the cache's answer there:
+// target = colour so far + throughput * radiance.  Paths that ended earlier
+// already wrote their targets.
+__global__ void k_cache_train_targets(const float4 *aux, const uint32_t *count, const float4 *radiance,
+                                      const float4 *t_color, const float4 *t_through, float4 *t_targets) {
+    const uint32_t nq = *count;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        uint32_t path = __float_as_uint(aux[2 * (size_t)q].w);
+        float3 c = mul_add(xyz(radiance[q]), xyz(t_through[path]), xyz(t_color[path]));
+        t_targets[path] = make_float4(c.x, c.y, c.z, 0.0f);
     }
 }
 
@@ -1555,9 +1570,47 @@ CacheArgs cache_args(const CacheFrame *cache) {
     return CA;
 }
 
+// The training paths queued in `in` (from the cache vertex on; A sinks
+// their radiance into the training targets): traced to max_depth, or -- with
+// a training suffix, in single-request frames -- `train_suffix` bounces on,
+// where the paths still going query the cache (with the training's current
+// weights, `weights`) and their targets take its answer.
+template <bool COUNT, bool BATCH>
+cudaError_t trace_training(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA, uint32_t in,
+                           const CacheFrame *cache, uint32_t max_depth, const uint8_t *weights) {
+    cudaError_t e;
+    const uint32_t K = cache->depth;
+    const bool short_paths = !BATCH && weights && cache->train_suffix && cache->s_count &&
+                             K + cache->train_suffix <= max_depth;
+    if (!short_paths) {
+        if (!L.split_extend) return tail_round<COUNT, BATCH>(L, A, in, K);
+        for (uint32_t depth = K; depth <= max_depth; depth++)
+            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+        return cudaSuccess;
+    }
+    const uint32_t last = K + cache->train_suffix;
+    for (uint32_t depth = K; depth < last; depth++)
+        if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+    CacheArgs SC = CA;
+    SC.features = cache->s_features;
+    SC.aux = cache->s_aux;
+    SC.count = cache->s_count;
+    if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
+    if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
+    if ((e = nrc::launch_infer(cache->s_features, cache->s_count, 0, cache->train_capacity, cache->s_radiance, weights,
+                               L.F->error_flags, L.stream)) != cudaSuccess)
+        return e;
+    uint32_t g = (cache->train_capacity + 255) / 256;
+    if (g > (uint32_t)(L.sms * 4)) g = (uint32_t)(L.sms * 4);
+    k_cache_train_targets<<<g ? g : 1, 256, 0, L.stream>>>(cache->s_aux, cache->s_count, cache->s_radiance,
+                                                            cache->t_color, cache->t_through, cache->t_targets);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // After the queries of a frame (or wave) are gathered: the training paths
-// traced on to max_depth, the Adam steps, the network's answers, and the
-// waiting paths resolved.
+// traced on (to max_depth, or a few bounces into the cache's own answers),
+// the Adam steps, the network's answers, and the waiting paths resolved.
 template <bool COUNT, bool BATCH>
 cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA, uint32_t &in, const CacheFrame *cache,
                         uint32_t max_depth) {
@@ -1603,13 +1656,8 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         TA.sink = cache->t_targets;
         TA.skip_glow_depth = cache->depth;
         TA.samples = TB.capacity;
-        if (!TL.split_extend) {
-            if ((e = tail_round<false, false>(TL, TA, 0, cache->depth)) != cudaSuccess) return e;
-        } else {
-            uint32_t tin = 0;
-            for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
-                if ((e = trace_round<false, false>(TL, TA, CA, tin, depth, false, false)) != cudaSuccess) return e;
-        }
+        if ((e = trace_training<false, false>(TL, TA, CA, 0, cache, max_depth, cache->train_weights)) != cudaSuccess)
+            return e;
         for (uint32_t off = 0; off < cache->train_capacity; off += cache->batch) {
             uint32_t n = cache->train_capacity - off < cache->batch ? cache->train_capacity - off : cache->batch;
             if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, ts)) !=
@@ -1630,12 +1678,9 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         A.path_throughput = cache->t_through;
         A.sink = cache->t_targets;
         A.skip_glow_depth = cache->depth;
-        if (!L.split_extend) {
-            if ((e = tail_round<COUNT, BATCH>(L, A, in, cache->depth)) != cudaSuccess) return e;
-        } else {
-            for (uint32_t depth = cache->depth; depth <= max_depth; depth++)
-                if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
-        }
+        if ((e = trace_training<COUNT, BATCH>(L, A, CA, in, cache, max_depth,
+                                              mode == SLIM_CACHE_ON ? cache->weights : nullptr)) != cudaSuccess)
+            return e;
         A = main;
     }
     if (train && !(cache->train_stream && cache->train_queues && !BATCH)) {

@@ -78,6 +78,14 @@ SCENE_DATA = _dt([("counts", (u4, 11), 0), ("flags", u2, 44), ("mesh_stack_size"
                   ("curves", u8, 128), ("aabbs", u8, 136), ("io", u8, 144), ("bvh_builder", u8, 152),
                   ("bvh_leaf_geometry_indices", u8, 160), ("bvh_nodes", u8, 168), ("bvh_node_count", u4, 176),
                   ("bvh_height", u1, 180)], 184)
+CAMERA = _dt([("orientation", (f4, 9), 0), ("rotation", (f4, 3), 36), ("position", (f4, 3), 48),
+              ("current_velocity", (f4, 3), 60), ("focal_length", f4, 72), ("zoom_amount", f4, 76),
+              ("target_distance", f4, 80), ("dolly_amount", f4, 84)], 88)
+SCENE_FILE = _dt([("counts", (u4, 11), 0), ("cameras", u8, 48), ("geometries", u8, 56), ("meshes", u8, 64),
+                  ("textures", u8, 72), ("grids", u8, 80), ("boxes", u8, 88), ("curves", u8, 96)], 104)
+GRID_BYTES, BOX_BYTES, CURVE_BYTES = 9700, 384, 12
+COUNT_GEOMETRIES, COUNT_CAMERAS, COUNT_LIGHTS, COUNT_MATERIALS, COUNT_TEXTURES, COUNT_MESHES = 0, 1, 2, 3, 4, 5
+COUNT_GRIDS, COUNT_BOXES, COUNT_TETS, COUNT_QUADS, COUNT_CURVES = 6, 7, 8, 9, 10
 CANVAS_DATA = _dt([("width_times_height", u4, 0), ("width_over_height", f4, 4), ("height_over_width", f4, 8),
                    ("f_width", f4, 12), ("f_height", f4, 16), ("h_width", f4, 20), ("h_height", f4, 24),
                    ("width", u2, 28), ("height", u2, 30), ("stride", u2, 32), ("antialias", i4, 36),
@@ -92,7 +100,7 @@ RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4,
                       ("radiance_cache", i4, 28), ("row_bands", i4, 32)], 36)
 CACHE_CONFIG = _dt([("cache_depth", u4, 0), ("train_samples", u4, 4), ("batch", u4, 8), ("seed", u4, 12),
                     ("learning_rate", f4, 16), ("beta1", f4, 20), ("beta2", f4, 24), ("epsilon", f4, 28),
-                    ("train", u4, 32), ("overlap", u4, 36), ("_reserved", (u4, 2), 40)], 48)
+                    ("train", u4, 32), ("overlap", u4, 36), ("train_suffix", u4, 40), ("_reserved", u4, 44)], 48)
 CACHE_STATS = _dt([("frames", u8, 0), ("steps", u8, 8), ("queries", u4, 16), ("train_samples", u4, 20),
                    ("loss", f4, 24), ("_pad", f4, 28)], 32)
 CACHE_OFF, CACHE_ON, CACHE_TRUNCATE, CACHE_EXACT = 0, 1, 2, 3
@@ -109,7 +117,6 @@ WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(
     ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",
      "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels"])], 80)
 STAGE_STATS = _dt([("name", "S24", 0), ("launches", u4, 24), ("total_ms", f4, 28), ("work", WORK_COUNTERS, 32)], 112)
-CAMERA = np.dtype([("orientation", f4, 9), ("position", f4, 3), ("focal_length", f4)])
 
 for _name, _dtype, _size in [("GEOMETRY", GEOMETRY, 72), ("MATERIAL", MATERIAL, 68), ("LIGHT", LIGHT, 32),
                              ("BVH_NODE", BVH_NODE, 32), ("TRIANGLE", TRIANGLE, 128), ("TEXEL_QUAD", TEXEL_QUAD, 12),

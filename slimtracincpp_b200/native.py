@@ -30,7 +30,7 @@ EXPORTS = [
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
     "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimSynchronize",
-    "slimGetLaunchCount", "slimPick", "slimDownloadSceneBVH",
+    "slimGetLaunchCount", "slimPick", "slimDownloadSceneBVH", "slimSaveScene", "slimReadSceneHeader", "slimLoadScene",
     "slimBatchSetRequests", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender",
 ]
 
@@ -74,6 +74,9 @@ def lib():
     h.slimReadTextureHeader.argtypes = [C.c_char_p, P, P]
     h.slimReadTexture.argtypes = [C.c_char_p, P, P, P]
     h.slimWriteTexture.argtypes = [C.c_char_p, P]
+    h.slimSaveScene.argtypes = [C.c_char_p, P]
+    h.slimReadSceneHeader.argtypes = [C.c_char_p, P, P]
+    h.slimLoadScene.argtypes = [C.c_char_p, P]
     h.slimBakeTexture.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
     h.slimBakeTextureOnGPU.argtypes = [P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P, P, P]
     h.slimGetStageStats.argtypes = [P, C.c_int, P]

@@ -19,11 +19,15 @@ from .native import check, lib, ptr
 class RadianceCache:
     @staticmethod
     def configure(cache_depth=2, train_samples=65536, batch=16384, seed=0, learning_rate=1e-2, beta1=0.9,
-                  beta2=0.99, epsilon=1e-8, train=True, overlap=True):
+                  beta2=0.99, epsilon=1e-8, train=True, overlap=True, train_suffix=0):
+        """train_suffix 0: training targets are full-depth paths traced by the
+        tracer; k > 0: training paths are traced k bounces on and end in the
+        cache's own answer (self-training)."""
         c = np.zeros((), L.CACHE_CONFIG)
         c["cache_depth"], c["train_samples"], c["batch"], c["seed"] = cache_depth, train_samples, batch, seed
         c["learning_rate"], c["beta1"], c["beta2"], c["epsilon"] = learning_rate, beta1, beta2, epsilon
         c["train"], c["overlap"] = int(bool(train)), int(bool(overlap))
+        c["train_suffix"] = int(train_suffix)
         check(lib().slimRadianceCacheConfigure(ptr(c)))
         return RadianceCache()
 

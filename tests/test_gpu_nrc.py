@@ -207,3 +207,34 @@ def test_cache_beats_truncation_after_online_training():
     p_trunc = psnr(to8(trunc, w.width, w.height), ref)
     assert scores[-1] > p_trunc + 3.0, (p_trunc, scores[0], scores[-1])
     assert scores[-1] > scores[0]
+
+
+@pytest.mark.parametrize("suffix", [1, 2])
+def test_self_training_cache_beats_truncation(suffix):
+    """Training paths traced `suffix` bounces past the cache vertex that end
+    in the cache's own answer there (the self-training targets): after online
+    training the cache frame is closer to the plain frame than cutting the
+    paths at vertex 2, and it improves as it trains."""
+    w = scenes.small_textured_scene(1, 128, 72, max_depth=6)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    plain, _ = r.render(vp)
+    ref = to8(plain, w.width, w.height)
+    cache = RadianceCache.configure(cache_depth=2, train_samples=4096, batch=512, seed=5, train_suffix=suffix)
+    assert int(cache.config()["train_suffix"]) == suffix
+    try:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_TRUNCATE)
+        trunc, _ = r.render(vp)
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
+        scores = []
+        for frame in range(120):
+            img, _ = r.render(vp, update_scene=False)
+            scores.append(psnr(to8(img, w.width, w.height), ref))
+        st = cache.stats()
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    assert st["train_samples"] > 0 and np.isfinite(st["loss"])
+    p_trunc = psnr(to8(trunc, w.width, w.height), ref)
+    assert scores[-1] > p_trunc + 3.0, (p_trunc, scores[0], scores[-1])
+    assert scores[-1] > scores[0]

@@ -13,6 +13,7 @@
 #      only users of the aliases (scene/camera.h) renamed to X/Y/Z.
 #   3. unqualified abs/sqrt/pow on floats: force-included ref/ref_shim.h
 #      (no source edit).
+#   (a fourth, for the bmp2texture tool only, is described where it is built)
 # Flags: -mfma so the reference's fast_mul_add is fmaf (FP_FAST_FMAF), and
 # -ffp-contract=off so nothing else is fused -- the floating-point policy the
 # CUDA kernels follow (-fmad=false with explicit fmaf at the same sites).
@@ -57,6 +58,25 @@ CXXFLAGS=(-std=c++17 -O3 -march=x86-64-v3 -mfma -ffp-contract=off -fno-fast-math
 g++ "${CXXFLAGS[@]}" -shared -o "$OUT/libslimref.so.tmp" "$HERE/ref/ref_driver.cpp"
 mv "$OUT/libslimref.so.tmp" "$OUT/libslimref.so"
 echo "built $OUT/libslimref.so"
+
+# The reference's texture converter (src/bmp2texture.cpp), unmodified, with
+# a Windows.h of the few Win32 calls it uses (ref/win32/Windows.h: stdio and
+# calloc underneath): oracle/_ref/bmp2texture, the checker of this library's
+# host and GPU texture bakers.
+cp "$REF_SRC/bmp2texture.cpp" "$TMP/bmp2texture.cpp"
+# 4. bmp2texture.cpp keeps its 2D mip loaders in a local `mips` and never
+#    sets `loader_mips`, which the final 8-bit pass then dereferences (null)
+#    for every texture that is not a cube map: as shipped the converter
+#    only bakes cube maps.  The one change the author evidently meant: the
+#    2D loaders are also `loader_mips`.
+sed -i 's/auto \*mips = new TextureMipLoader\[texture.mip_count\];/auto *mips = loader_mips = new TextureMipLoader[texture.mip_count];/' \
+    "$TMP/bmp2texture.cpp"
+grep -q 'auto \*mips = loader_mips = new TextureMipLoader' "$TMP/bmp2texture.cpp"
+g++ -std=c++17 -O2 -DNDEBUG -march=x86-64-v3 -mfma -ffp-contract=off -fno-fast-math -w \
+    -include "$HERE/ref/ref_shim.h" -I "$HERE/ref/win32" -I "$TMP" \
+    -o "$OUT/bmp2texture.tmp" "$TMP/bmp2texture.cpp"
+mv "$OUT/bmp2texture.tmp" "$OUT/bmp2texture"
+echo "built $OUT/bmp2texture"
 
 # The timed CPU baseline: the same sources with plain release flags
 # (-O3 -DNDEBUG, the compiler's default contraction, no parity flags).  The

@@ -673,7 +673,7 @@ def run_batch_bench(args, torch, dist, dev, rank, world, local):
     single_ms = []
     for q, ptr in zip(reqs, ptrs):
         batch.set_requests([q], [ptr])
-        batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"])
+        batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"], plan["persistent"])
         batch.render(sp)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)

@@ -242,7 +242,7 @@ SLIM_STATIC_ASSERT(sizeof(SlimRenderOptions) == 36, "RenderOptions is 36 bytes")
  * Drop-in hooks (renderer/renderer_GPU.h)                                   *
  * ======================================================================== */
 
-/* Replaces initDataOnGPU(const Scene&) (renderer/renderer_GPU.h:180-281):
+/* Replaces initDataOnGPU(const Scene&) (renderer/renderer_GPU.h:80-181):
  * one-time deep copy of the scene -- geometries, materials, lights, scene
  * BVH, meshes (triangles + BVH nodes) and textures (mips + texel quads) --
  * into the device layout.  Mesh and texture topology is frozen afterwards,
@@ -250,7 +250,7 @@ SLIM_STATIC_ASSERT(sizeof(SlimRenderOptions) == 36, "RenderOptions is 36 bytes")
 int slimInitDataOnGPU(const SlimSceneData *scene);
 
 /* Replace uploadLights/uploadCameras/uploadGeometries/uploadMaterials/
- * uploadSceneBVH(const Scene&) (renderer/renderer_GPU.h:170-178): re-upload
+ * uploadSceneBVH(const Scene&) (renderer/renderer_GPU.h:70-78): re-upload
  * the per-frame mutable parts.  Counts must equal those given to
  * slimInitDataOnGPU (SLIM_ERR_STATE otherwise). */
 int slimUploadLights(const SlimSceneData *scene);
@@ -260,7 +260,7 @@ int slimUploadMaterials(const SlimSceneData *scene);
 int slimUploadSceneBVH(const SlimSceneData *scene);
 
 /* Replaces renderOnGPU(const Canvas&, const CameraRayProjection&,
- * const RayTracerSettings&) (renderer/renderer_GPU.h:148-168): traces every
+ * const RayTracerSettings&) (renderer/renderer_GPU.h:48-68): traces every
  * pixel (every sub-sample under SSAA) and writes canvas->pixels (Pixel
  * {clamp(c)^2, 1}) and canvas->depths synchronously, like the reference.
  * Into pinned host memory (cudaHostAlloc) the rows download while later
@@ -458,6 +458,11 @@ typedef struct {
     uint32_t candidates;       /* out: plans the tuner timed */
     uint32_t graph_nodes;      /* out: kernel nodes of the captured graph (0 before the first render) */
     uint32_t tuned;            /* out: non-zero when slimBatchTune chose the plan */
+    uint32_t persistent;       /* non-zero: the requests without the radiance cache are rendered by
+                                  one persistent launch that pulls their pixels from a device work
+                                  queue (warps refill finished paths), beside the waves of the
+                                  requests with the cache; 0: every request goes through the waves */
+    uint32_t _pad;
 } SlimBatchPlan;
 
 /* Uploads the requests (validated like slimInitDataOnGPU) and drops any
@@ -476,7 +481,7 @@ int slimBatchRender(void *stream);
 SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheConfig) == 48, "RadianceCacheConfig is 48 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheStats) == 32, "RadianceCacheStats is 32 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRenderRequest) == 184, "RenderRequest is 184 bytes");
-SLIM_STATIC_ASSERT(sizeof(SlimBatchPlan) == 32, "BatchPlan is 32 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimBatchPlan) == 40, "BatchPlan is 40 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimPick) == 32, "Pick is 32 bytes");
 
 /* Host-side helpers: the reference's own host algorithms, restated. */

@@ -42,9 +42,12 @@ class BatchRenderer:
         check(lib().slimBatchTune(int(stream)))
         return self.plan()
 
-    def set_plan(self, queue_capacity, tile_pixels, block_size=256):
+    def set_plan(self, queue_capacity, tile_pixels, block_size=256, persistent=False):
+        """persistent: the requests without the radiance cache render in one
+        persistent launch fed by a device pixel queue (the others in waves)."""
         p = np.zeros((), L.BATCH_PLAN)
         p["queue_capacity"], p["tile_pixels"], p["block_size"] = queue_capacity, tile_pixels, block_size
+        p["persistent"] = int(bool(persistent))
         check(lib().slimBatchSetPlan(ptr(p)))
 
     def plan(self):

@@ -1703,6 +1703,10 @@ struct BatchState {
     DevArray<DevFrame> frames;
     DevArray<uint4> tiles;
     std::vector<uint4> h_tiles;
+    // persistent plan: the requests rendered by the persistent launch and the
+    // first pixel of each in its flattened pixel queue
+    DevArray<uint32_t> p_requests, p_prefix, p_cursor;
+    uint32_t p_count = 0, p_total = 0;
     std::vector<BatchWave> waves;
     uint64_t pixels = 0;
     uint32_t max_lights = 0, max_instances = 0;
@@ -1766,9 +1770,17 @@ int plan_waves(BatchState &b) {
         slot = 0;
     };
     close();
+    std::vector<uint32_t> preq, prefix;
+    uint64_t ptotal = 0;
     for (uint32_t r = 0; r < b.requests.size(); r++) {
         const SlimRenderRequest &q = b.requests[r];
         const uint32_t n = q.width * q.height;
+        if (b.plan.persistent && !b.h_frames[r].cache_depth) {   // the persistent launch renders it
+            preq.push_back(r);
+            prefix.push_back((uint32_t)ptotal);
+            ptotal += n;
+            continue;
+        }
         for (uint32_t first = 0; first < n; first += T) {
             uint32_t count = n - first < T ? n - first : T;
             if (slot + count > Q) close();
@@ -1783,8 +1795,18 @@ int plan_waves(BatchState &b) {
         }
     }
     close();
+    if (ptotal > 0xFFFFFFFFull - 4096) return set_error(SLIM_ERR_LIMIT, "persistent batch of 2^32 pixels or more");
     int rc = b.tiles.reserve(b.h_tiles.size() ? b.h_tiles.size() : 1, "alloc batch tiles");
     if (rc) return rc;
+    b.p_count = (uint32_t)preq.size();
+    b.p_total = (uint32_t)ptotal;
+    if ((rc = b.p_requests.reserve(preq.size() ? preq.size() : 1, "alloc persistent batch table"))) return rc;
+    if ((rc = b.p_prefix.reserve(prefix.size() ? prefix.size() : 1, "alloc persistent batch table"))) return rc;
+    if ((rc = b.p_cursor.reserve(1, "alloc persistent batch cursor"))) return rc;
+    if (!preq.empty()) {
+        SLIM_CUDA(cudaMemcpy(b.p_requests.ptr, preq.data(), preq.size() * 4, cudaMemcpyHostToDevice), "upload persistent batch table");
+        SLIM_CUDA(cudaMemcpy(b.p_prefix.ptr, prefix.data(), prefix.size() * 4, cudaMemcpyHostToDevice), "upload persistent batch table");
+    }
     if (!b.h_tiles.empty())
         SLIM_CUDA(cudaMemcpy(b.tiles.ptr, b.h_tiles.data(), b.h_tiles.size() * sizeof(uint4), cudaMemcpyHostToDevice),
                   "upload batch tiles");
@@ -1889,6 +1911,11 @@ int batch_launch(Context &c, BatchState &b, cudaStream_t stream) {
     BF.lane_queues = &b.q[1].B;
     BF.lane_fork = b.lane_fork;
     BF.lane_join = b.lane_join;
+    BF.p_requests = b.p_requests.ptr;
+    BF.p_prefix = b.p_prefix.ptr;
+    BF.p_count = b.p_count;
+    BF.p_total = b.p_total;
+    BF.p_cursor = b.p_cursor.ptr;
     cudaError_t e = launch_render_batch(BF, b.q[0].B, b.plan.block_size, stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "batch launch");
     return SLIM_OK;
@@ -2078,6 +2105,7 @@ int slimBatchSetPlan(const SlimBatchPlan *plan) {
     b.plan.queue_capacity = plan->queue_capacity;
     b.plan.tile_pixels = plan->tile_pixels;
     b.plan.block_size = plan->block_size;
+    b.plan.persistent = plan->persistent ? 1u : 0u;
     b.plan.tuned = 0;
     b.plan.batch_ms = 0;
     b.plan.candidates = 0;
@@ -2107,10 +2135,11 @@ int slimBatchTune(void *stream) {
     if (!best.queue_capacity) { best.queue_capacity = 4u << 20; best.tile_pixels = 1u << 16; best.block_size = 256; }
     float best_ms = 1e30f;
     uint32_t tried = 0;
-    auto attempt = [&](uint32_t Q, uint32_t T, int block) -> int {
+    auto attempt = [&](uint32_t Q, uint32_t T, int block, uint32_t persistent = 0) -> int {
         b.plan.queue_capacity = Q;
         b.plan.tile_pixels = T;
         b.plan.block_size = block;
+        b.plan.persistent = persistent;
         float ms = 0;
         int rc = batch_time(c, b, s, 2, ms);
         if (rc) return rc;
@@ -2133,6 +2162,16 @@ int slimBatchTune(void *stream) {
         if (block != best.block_size && (rc = attempt(best.queue_capacity, best.tile_pixels, block))) return fail(rc);
     for (uint32_t T : {1u << 14, 1u << 18})
         if ((rc = attempt(best.queue_capacity, T, best.block_size))) return fail(rc);
+    // the requests without the cache in one persistent launch instead of waves
+    bool plain = false;
+    for (const DevFrame &f : b.h_frames) plain = plain || !f.cache_depth;
+    if (plain) {
+        const SlimBatchPlan waves_best = best;
+        if ((rc = attempt(waves_best.queue_capacity, waves_best.tile_pixels, waves_best.block_size, 1))) return fail(rc);
+        for (uint32_t Q : {1u << 20, 4u << 20})   // the waves left are the cache requests' alone
+            if (Q != waves_best.queue_capacity && (rc = attempt(Q, waves_best.tile_pixels, waves_best.block_size, 1)))
+                return fail(rc);
+    }
     b.plan = best;
     b.plan.batch_ms = best_ms;
     b.plan.candidates = tried;

@@ -147,9 +147,22 @@ struct BatchFrame {
     cudaStream_t lane_stream;
     const WavefrontBuffers *lane_queues;
     cudaEvent_t lane_fork, lane_join;
+    // Requests without the cache in one persistent launch (plan.persistent):
+    // their pixels are in no wave; the launch runs on the second lane (or
+    // first, before the waves, with one lane) beside the cache requests' waves.
+    const uint32_t *p_requests, *p_prefix;
+    uint32_t p_count, p_total;
+    uint32_t *p_cursor;
 };
 cudaError_t launch_render_batch(const BatchFrame &BF, const WavefrontBuffers &B, int block, cudaStream_t stream,
                                 StageTimer *timer);
+// Every pixel of the listed requests (prefix[k] = first pixel of request
+// requests[k] in one flattened queue of `total` pixels) rendered by one
+// persistent launch (kernels_fused.cu k_batch_persistent); `cursor` is a
+// device counter the launch clears first.
+cudaError_t launch_batch_persistent(const DevScene *scenes, const DevFrame *frames, const uint32_t *requests,
+                                    const uint32_t *prefix, uint32_t count, uint32_t total, uint32_t *cursor,
+                                    uint32_t *error_flags, unsigned long long *counters, cudaStream_t stream);
 
 // GPU refit of the scene BVH: recomputes every node's bounds bottom-up from
 // the geometries' world AABBs, keeping the uploaded topology.

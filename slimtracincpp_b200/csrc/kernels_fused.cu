@@ -9,16 +9,103 @@ namespace slim {
 namespace dev {
 
 template <bool COUNT>
-SLIM_D void flush_work(const DevFrame &F, const Work &w) {
-    if (!COUNT || !F.counters) return;
+SLIM_D void flush_work(unsigned long long *counters, const Work &w) {
+    if (!COUNT || !counters) return;
     uint32_t v[9] = {w.primary, w.shadow, w.bounce, w.scene_nodes, w.mesh_nodes, w.triangles,
                      w.geometries, w.mesh_fetches, w.taps};
 #pragma unroll
     for (int k = 0; k < 9; k++) {
         unsigned long long s = v[k];
         for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
-        if ((threadIdx.x & 31) == 0 && s) atomicAdd(F.counters + k, s);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(counters + k, s);
     }
+}
+
+// renderPixelBeauty (renderer/ray_tracer.h:19-108) as a sequence of path
+// segments: a path's state between two segments is the ray of the next one,
+// the colour and throughput so far, the canvas depth and the bounces left.
+struct PathState {
+    float3 o, d;
+    float3 color, throughput;
+    float depth, scaling;
+    uint32_t depth_left;
+};
+
+template <bool COUNT>
+SLIM_D void path_start(const DevFrame &F, int x, int y, PathState &p, Work &w) {
+    const SlimCameraRayProjection &P = F.projection;
+    p.scaling = F.cones_per_pixel ? pixel_scaling(P, x, y) : 0.0f;
+    p.o = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
+    p.d = normalized(primary_direction(P, x, y));
+    bump<COUNT>(w.primary);
+    p.color = f3(0, 0, 0);
+    p.throughput = f3(1, 1, 1);
+    p.depth = INFINITY;
+    p.depth_left = F.settings.max_depth;
+}
+
+// One segment: closest hit, shading (point lights with their shadow rays,
+// area lights, IBL), the bounce decision, the light glow of the segment.
+// Returns whether the path goes on.
+template <bool COUNT>
+SLIM_D bool path_segment(const DevScene &S, const DevFrame &F, PathState &p, uint32_t *stack, uint32_t *mesh_stack,
+                         uint32_t &err, Work &w) {
+    const SlimRayTracerSettings &st = F.settings;
+    Ray ray;
+    reset(ray, p.o, p.d);
+    Hit hit;
+    Surface s;
+    float3 current = f3(0, 0, 0), next_throughput = f3(0, 0, 0);
+    int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+    if (g >= 0) {
+        Geo geo = load_geo(S, (uint32_t)g);
+        Mat m = load_mat(S, geo.material);
+        if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+            p.depth_left = 0;
+            current = m.emission;
+        } else {
+            prepare_for_shading<COUNT>(S, geo, m, ray, hit, p.scaling, s, w);
+            if (p.depth_left == st.max_depth) p.depth = depth_at(F.projection, hit.position);
+            for (uint32_t i = 0; i < S.light_count; i++) {
+                LightRec l = load_light(S, i);
+                if (!is_facing_light(s, l)) continue;
+                if (l.flags & SLIM_LIGHT_IS_SHADOWING) {
+                    Ray sr;
+                    sr.o = s.P;
+                    sr.d = s.L;
+                    Hit sh;
+                    bump<COUNT>(w.shadow);
+                    if (scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0) continue;
+                }
+                add_light(s, m, l, current);
+            }
+            if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
+            if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
+                s.L = s.N;
+                s.NdotL = 1.0f;
+                float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
+                float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
+                radiance_fraction(s, m);
+                current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
+            }
+            if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && --p.depth_left) {
+                float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
+                next_throughput = s.refracted ? one_minus(Fr) : Fr;
+                reset(ray, hit.position, s.RF);
+                bump<COUNT>(w.bounce);
+            } else p.depth_left = 0;
+        }
+    } else {
+        p.depth_left = 0;
+        if (st.skybox_color_texture_id >= 0)
+            current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
+    }
+    add_glow(S, ray, hit.distance, current);
+    p.color = mul_add(current, p.throughput, p.color);
+    p.throughput = p.throughput * next_throughput;
+    p.o = ray.o;
+    p.d = ray.d;
+    return p.depth_left != 0;
 }
 
 // renderPixelBeauty / renderPixelDebugMode for one sample.
@@ -27,16 +114,16 @@ SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, ui
                           uint32_t *mesh_stack, uint32_t &err, Work &w, float3 &out_color, float &out_depth) {
     const SlimCameraRayProjection &P = F.projection;
     const SlimRayTracerSettings &st = F.settings;
-    float scaling = F.cones_per_pixel ? pixel_scaling(P, x, y) : 0.0f;
-    float3 cam = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
-    Ray ray;
-    reset(ray, cam, normalized(primary_direction(P, x, y)));
-    Hit hit;
-    bump<COUNT>(w.primary);
-    float3 color = f3(0, 0, 0);
-    float depth = INFINITY;
-    Surface s;
     if (st.render_mode != SLIM_RENDER_BEAUTY) {
+        float scaling = F.cones_per_pixel ? pixel_scaling(P, x, y) : 0.0f;
+        float3 cam = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
+        Ray ray;
+        reset(ray, cam, normalized(primary_direction(P, x, y)));
+        Hit hit;
+        bump<COUNT>(w.primary);
+        float3 color = f3(0, 0, 0);
+        float depth = INFINITY;
+        Surface s;
         int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
         if (g >= 0) {
             Geo geo = load_geo(S, (uint32_t)g);
@@ -66,60 +153,11 @@ SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, ui
         out_depth = depth;
         return;
     }
-    float3 throughput = f3(1, 1, 1), next_throughput = f3(0, 0, 0);
-    uint32_t depth_left = st.max_depth;
-    while (depth_left) {
-        float3 current = f3(0, 0, 0);
-        int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
-        if (g >= 0) {
-            Geo geo = load_geo(S, (uint32_t)g);
-            Mat m = load_mat(S, geo.material);
-            if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
-                depth_left = 0;
-                current = m.emission;
-            } else {
-                prepare_for_shading<COUNT>(S, geo, m, ray, hit, scaling, s, w);
-                if (depth_left == st.max_depth) depth = depth_at(P, hit.position);
-                for (uint32_t i = 0; i < S.light_count; i++) {
-                    LightRec l = load_light(S, i);
-                    if (!is_facing_light(s, l)) continue;
-                    if (l.flags & SLIM_LIGHT_IS_SHADOWING) {
-                        Ray sr;
-                        sr.o = s.P;
-                        sr.d = s.L;
-                        Hit sh;
-                        bump<COUNT>(w.shadow);
-                        if (scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0) continue;
-                    }
-                    add_light(s, m, l, current);
-                }
-                if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
-                if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
-                    s.L = s.N;
-                    s.NdotL = 1.0f;
-                    float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
-                    float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
-                    radiance_fraction(s, m);
-                    current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
-                }
-                if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && --depth_left) {
-                    float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
-                    next_throughput = s.refracted ? one_minus(Fr) : Fr;
-                    reset(ray, hit.position, s.RF);
-                    bump<COUNT>(w.bounce);
-                } else depth_left = 0;
-            }
-        } else {
-            depth_left = 0;
-            if (st.skybox_color_texture_id >= 0)
-                current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
-        }
-        add_glow(S, ray, hit.distance, current);
-        color = mul_add(current, throughput, color);
-        throughput = throughput * next_throughput;
-    }
-    out_color = f3(tone_mapped_baked(color.x), tone_mapped_baked(color.y), tone_mapped_baked(color.z));
-    out_depth = depth;
+    PathState p;
+    path_start<COUNT>(F, x, y, p, w);
+    while (p.depth_left && path_segment<COUNT>(S, F, p, stack, mesh_stack, err, w)) {}
+    out_color = f3(tone_mapped_baked(p.color.x), tone_mapped_baked(p.color.y), tone_mapped_baked(p.color.z));
+    out_depth = p.depth;
 }
 
 template <bool COUNT>
@@ -136,7 +174,67 @@ __global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
         set_pixel(F, x, y, color, depth);
         if (err) atomicOr(F.error_flags, err);
     }
-    flush_work<COUNT>(F, w);
+    flush_work<COUNT>(F.counters, w);
+}
+
+// ---- batched requests in one persistent launch -------------------------------
+// The pixels of the requests listed in `requests` form one work queue: pixel
+// f of it belongs to request requests[k] with prefix[k] <= f < prefix[k + 1]
+// (pixel f - prefix[k] of that request in 8 x 4 tile order).  Every warp
+// keeps 32 paths in flight: each turn every live lane traces one path segment
+// (closest hit, shading with its shadow rays, bounce), a lane whose path
+// ended writes its pixel, and the idle lanes of the warp claim the next
+// pixels of the queue together (one atomic per warp, ranks by ballot), so
+// warps stay full until the queue is empty whatever the path lengths.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_batch_persistent(const DevScene *scenes, const DevFrame *frames,
+                                                          const uint32_t *requests, const uint32_t *prefix,
+                                                          uint32_t count, uint32_t total, uint32_t *cursor,
+                                                          uint32_t *error_flags, unsigned long long *counters) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    PathState p;
+    bool live = false;
+    uint32_t req = 0, x = 0, y = 0;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xFFFFFFFFu, !live);
+        if (idle) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(cursor, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (!live) {
+                const uint32_t f = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+                if (base < total && f < total) {
+                    uint32_t lo = 0, hi = count;          // last k with prefix[k] <= f
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (__ldg(prefix + mid) <= f) lo = mid; else hi = mid;
+                    }
+                    req = __ldg(requests + lo);
+                    const DevFrame &F = frames[req];
+                    const uint32_t pixel = pixel_of_slot(F.width, F.height, f - __ldg(prefix + lo));
+                    x = pixel % F.width;
+                    y = pixel / F.width;
+                    path_start<COUNT>(F, (int)x, (int)y, p, w);
+                    live = true;
+                }
+            }
+            if (!__any_sync(0xFFFFFFFFu, live)) break;
+        }
+        if (live) {
+            const DevFrame &F = frames[req];
+            if (!p.depth_left || !path_segment<COUNT>(scenes[req], F, p, stack, mesh_stack, err, w)) {
+                set_pixel(F, (int)x, (int)y,
+                          f3(tone_mapped_baked(p.color.x), tone_mapped_baked(p.color.y), tone_mapped_baked(p.color.z)),
+                          p.depth);
+                live = false;
+            }
+        }
+    }
+    if (err) atomicOr(error_flags, err);
+    flush_work<COUNT>(counters, w);
 }
 
 // First closest hit of each primary ray (renderer/ray_tracer.h:36-45).
@@ -236,6 +334,28 @@ cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block,
         count_launch();
     }
     if (timer) timer->end(STAGE_FUSED, stream);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_persistent(const DevScene *scenes, const DevFrame *frames, const uint32_t *requests,
+                                    const uint32_t *prefix, uint32_t count, uint32_t total, uint32_t *cursor,
+                                    uint32_t *error_flags, unsigned long long *counters, cudaStream_t stream) {
+    if (!count || !total) return cudaSuccess;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaMemsetAsync(cursor, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    if (counters) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_batch_persistent<true>, 128, 0);
+        dev::k_batch_persistent<true><<<sms * (per_sm > 0 ? per_sm : 1), 128, 0, stream>>>(
+            scenes, frames, requests, prefix, count, total, cursor, error_flags, counters);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::k_batch_persistent<false>, 128, 0);
+        dev::k_batch_persistent<false><<<sms * (per_sm > 0 ? per_sm : 1), 128, 0, stream>>>(
+            scenes, frames, requests, prefix, count, total, cursor, error_flags, counters);
+    }
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -150,29 +150,6 @@ SLIM_D void primary_ray(const DevFrame &F, uint32_t i, float3 &o, float3 &d) {
     d = normalized(primary_direction(P, x, y));
 }
 
-// Primary rays are numbered in 8 x 4 pixel tiles, so the 32 rays of a warp
-// (and the shadow rays and hits that follow them through the queues) cover
-// a compact patch instead of a 32-pixel row strip: within every band of 4
-// rows the slots run through 8-column groups; the columns past the last
-// full group, and a last band shorter than 4 rows, keep row order.  A
-// bijection of [0, width * height); config 2: 2.08 -> 2.03 ms.
-SLIM_D uint32_t pixel_of_slot(uint32_t W, uint32_t H, uint32_t slot) {
-    const uint32_t band = 4u * W;
-    const uint32_t b = slot / band;
-    if (b >= H / 4u) return slot;
-    const uint32_t j = slot - b * band;
-    const uint32_t groups = W / 8u, g = j / 32u;
-    uint32_t x, y;
-    if (g < groups) {
-        x = g * 8u + (j & 7u);
-        y = b * 4u + ((j & 31u) >> 3);
-    } else {
-        const uint32_t r = j - groups * 32u, rest = W - groups * 8u;
-        x = groups * 8u + r % rest;
-        y = b * 4u + r / rest;
-    }
-    return y * W + x;
-}
 
 SLIM_D void load_ray(const DevFrame &F, const QueueArgs &A, uint32_t slot, float3 &o, float3 &d, uint32_t &path,
                      uint32_t &pid) {
@@ -1795,10 +1772,21 @@ cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B0, int bloc
         if ((e = cudaStreamWaitEvent(BF.lane_stream, BF.lane_fork, 0)) != cudaSuccess) return e;
     }
     uint32_t next_lane = 0;
+    if (BF.p_count && BF.p_total) {
+        // the persistent launch takes the second lane; the waves (the cache
+        // requests') all stay on the first
+        cudaStream_t ps = two_lanes ? BF.lane_stream : stream0;
+        if (timer) timer->begin(STAGE_FUSED, ps);
+        if ((e = launch_batch_persistent(BF.scenes, BF.frames, BF.p_requests, BF.p_prefix, BF.p_count, BF.p_total,
+                                         BF.p_cursor, BF.frame.error_flags, BF.frame.counters, ps)) != cudaSuccess)
+            return e;
+        if (timer) timer->end(STAGE_FUSED, ps);
+    }
+    const bool one_lane_waves = BF.p_count && BF.p_total;
     for (uint32_t wi = 0; wi < BF.wave_count; wi++) {
         const BatchWave &wave = BF.waves[wi];
         uint32_t lane = 0;
-        if (two_lanes && !(cache && wave.cache_paths)) {
+        if (two_lanes && !one_lane_waves && !(cache && wave.cache_paths)) {
             lane = next_lane;
             next_lane ^= 1u;
         }

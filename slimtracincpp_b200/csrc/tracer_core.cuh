@@ -961,6 +961,30 @@ SLIM_D float3 primary_direction(const SlimCameraRayProjection &p, int x, int y) 
     float3 right = f3(p.right.x, p.right.y, p.right.z);
     return (start + down * (float)y) + right * (float)x;
 }
+// Primary rays are numbered in 8 x 4 pixel tiles, so the 32 rays of a warp
+// (and the shadow rays and hits that follow them through the queues) cover
+// a compact patch instead of a 32-pixel row strip: within every band of 4
+// rows the slots run through 8-column groups; the columns past the last
+// full group, and a last band shorter than 4 rows, keep row order.  A
+// bijection of [0, width * height); config 2: 2.08 -> 2.03 ms.
+SLIM_D uint32_t pixel_of_slot(uint32_t W, uint32_t H, uint32_t slot) {
+    const uint32_t band = 4u * W;
+    const uint32_t b = slot / band;
+    if (b >= H / 4u) return slot;
+    const uint32_t j = slot - b * band;
+    const uint32_t groups = W / 8u, g = j / 32u;
+    uint32_t x, y;
+    if (g < groups) {
+        x = g * 8u + (j & 7u);
+        y = b * 4u + ((j & 31u) >> 3);
+    } else {
+        const uint32_t r = j - groups * 32u, rest = W - groups * 8u;
+        x = groups * 8u + r % rest;
+        y = b * 4u + r / rest;
+    }
+    return y * W + x;
+}
+
 SLIM_D float pixel_scaling(const SlimCameraRayProjection &p, int x, int y) {
     float cx = fmaf((float)x, p.sample_size, p.C_start.x);
     float cy = fmaf((float)-y, p.sample_size, p.C_start.y);

@@ -110,7 +110,8 @@ RENDER_REQUEST = _dt([("scene", u8, 0), ("projection", PROJECTION, 8), ("setting
 PICK = _dt([("geometry", i4, 0), ("light", i4, 4), ("triangle", u4, 8), ("distance", f4, 12),
             ("position", (f4, 3), 16), ("from_behind", u4, 28)], 32)
 BATCH_PLAN = _dt([("queue_capacity", u4, 0), ("tile_pixels", u4, 4), ("block_size", i4, 8), ("waves", u4, 12),
-                  ("batch_ms", f4, 16), ("candidates", u4, 20), ("graph_nodes", u4, 24), ("tuned", u4, 28)], 32)
+                  ("batch_ms", f4, 16), ("candidates", u4, 20), ("graph_nodes", u4, 24), ("tuned", u4, 28),
+                  ("persistent", u4, 32), ("_pad", u4, 36)], 40)
 NRC_PARAMS = 18624
 NRC_FEATURES = 16
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(

@@ -167,3 +167,44 @@ def test_config5_shaped_batch_matches_oracle():
     got = render_batch(BatchRenderer(assets(mesh_assets)), plain)
     for q, (pix, dep) in zip(plain, got):
         _assert_matches_oracle(q, pix, dep)
+
+
+def test_persistent_batch_matches_oracle_and_fused_frames(meshes):
+    """The persistent plan: every request without the cache is rendered by
+    one persistent launch fed by a device pixel queue (warps refill lanes
+    whose paths ended).  Its per-path arithmetic is the fused engine's, so
+    each request equals its single frame rendered by the fused engine bit
+    for bit, and the oracle within the usual bars; two replays of the
+    captured graph change nothing."""
+    reqs = make_requests(meshes, 6, 9)
+    batch = BatchRenderer(assets(meshes))
+    got = render_batch(batch, reqs, plan=(1 << 16, 4096, 256, True), repeats=2)
+    plan = batch.plan()
+    assert plan["persistent"] == 1 and plan["waves"] == 0
+    for q, (pix, dep) in zip(reqs, got):
+        native.set_render_options(engine=L.ENGINE_MEGAKERNEL)
+        r = RayTracingRenderer(q.scene, int(q.settings["max_depth"]))
+        spix, sdep = r.render(Viewport(q.camera, q.width, q.height))
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+        assert np.array_equal(pix.view(np.uint32), spix.view(np.uint32)), q.name
+        assert np.array_equal(dep.view(np.uint32), sdep.view(np.uint32)), q.name
+        _assert_matches_oracle(q, pix, dep)
+
+
+def test_persistent_plan_beside_cache_waves(meshes):
+    """Cache requests keep their waves while the plain requests run in the
+    persistent launch on the second lane: the plain requests still match
+    the wave plan's output bit for bit."""
+    reqs = make_requests(meshes, 7, 6, cache_every=2)
+    RadianceCache.configure(cache_depth=2, train_samples=2048, batch=1024, seed=3)
+    batch = BatchRenderer(assets(meshes))
+    a = render_batch(batch, reqs, plan=(1 << 16, 4096, 256, True))
+    assert batch.plan()["waves"] >= 1
+    for q, (pix, dep) in zip(reqs, a):
+        assert np.isfinite(pix).all()
+        if q.radiance_cache == L.CACHE_OFF:
+            native.set_render_options(engine=L.ENGINE_MEGAKERNEL)
+            r = RayTracingRenderer(q.scene, int(q.settings["max_depth"]))
+            spix, _ = r.render(Viewport(q.camera, q.width, q.height))
+            native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+            assert np.array_equal(pix.view(np.uint32), spix.view(np.uint32)), q.name

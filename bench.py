@@ -205,6 +205,40 @@ def algorithmic_bytes(w, pixels=None):
             64 * w["mesh_hit_fetches"] + 72 * w["geometry_tests"] + 16 * w["texel_taps"] + 20 * fb)
 
 
+def reference_order_stage_bytes(w):
+    """Algorithmic bytes of one frame split by wavefront stage, from the fused
+    engine's counters (every ray walked in the reference's order, any-hit
+    traversal work counted apart): extend = the closest-hit walks (scene and
+    mesh nodes, triangles, instances, hit attribute fetches), shadow = the
+    any-hit walks' scene nodes and instances, shadow_mesh = their mesh nodes
+    and triangles."""
+    if "shadow_scene_node_tests" not in w:
+        return {}
+    closest_nodes = w["scene_node_tests"] + w["mesh_node_tests"] - w["shadow_scene_node_tests"] - w["shadow_mesh_node_tests"]
+    return {"extend": 32 * closest_nodes + 64 * (w["triangle_tests"] - w["shadow_triangle_tests"]) +
+                      64 * w["mesh_hit_fetches"] + 72 * (w["geometry_tests"] - w["shadow_geometry_tests"]),
+            "shadow": 32 * w["shadow_scene_node_tests"] + 72 * w["shadow_geometry_tests"],
+            "shadow_mesh": 32 * w["shadow_mesh_node_tests"] + 64 * w["shadow_triangle_tests"]}
+
+
+def l2_copy_gbs(torch, dev, mib=24, reps=200):
+    """L2 bandwidth of a plain device-to-device copy whose source and
+    destination (2 x `mib` MiB) stay in the 126 MB L2: read + write bytes
+    over CUDA-event time."""
+    n = (mib << 20) // 4
+    src = torch.ones(n, dtype=torch.float32, device=dev)
+    dst = torch.empty_like(src)
+    for _ in range(10):
+        dst.copy_(src)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        dst.copy_(src)
+    b.record()
+    torch.cuda.synchronize()
+    return 2.0 * (mib << 20) * reps / (a.elapsed_time(b) / 1000.0) / 1e9
+
+
 # DRAM bytes (read + write) per launch of a stage, measured with
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
 # on the bench's own command (profiles/ holds the per-kernel table).  ncu flushes caches before every kernel, so
@@ -846,16 +880,28 @@ def main():
         d = timed[dom_name]
         per_launch_ms = d["total_ms"] / d["launches"]
         launches_per_frame = d["launches"] / args.steps
-        px = work["primary_rays"] if dom_name in PIXEL_STAGES else 0
-        alg = algorithmic_bytes(stage_work[dom_name], px) / max(1.0, launches_per_frame)
+        ref_bytes = reference_order_stage_bytes(work)
+        if dom_name in ref_bytes:
+            alg_frame, alg_source = ref_bytes[dom_name], "reference-order counts (fused engine), this stage's part"
+        else:
+            px = work["primary_rays"] if dom_name in PIXEL_STAGES else 0
+            alg_frame, alg_source = algorithmic_bytes(stage_work[dom_name], px), "the stage's own counters"
+        alg = alg_frame / max(1.0, launches_per_frame)
         achieved = alg / (per_launch_ms / 1000.0) / 1e9
+        l2_peak = l2_copy_gbs(torch, dev)
         roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                     "traffic": TRAFFIC_BYTES_PER_LAUNCH.get((args.config, dom_name)),
                     "traffic_note": "ncu dram read+write per stage launch, cold caches",
-                    "algorithmic_bytes_per_launch": alg, "ms_per_launch": per_launch_ms,
+                    "algorithmic_bytes_per_launch": alg, "algorithmic_bytes_source": alg_source,
+                    "ms_per_launch": per_launch_ms,
                     "share_of_frame": d["total_ms"] / prof_ms,
-                    "timing": "CUDA events around every launch of the stage, whole-frame passes (row_bands=1)"}
+                    "timing": "CUDA events around every launch of the stage, whole-frame passes (row_bands=1)",
+                    "l2": {"achieved": achieved, "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak,
+                           "peak_source": "measured here: device-to-device copy of 2 x 24 MiB, L2-resident "
+                                          "(read + write bytes over CUDA-event time)",
+                           "note": "the scene's nodes and triangles (34 MB) stay in the 126 MB L2; the stage's "
+                                   "algorithmic bytes are mostly L1/L2 traffic"}}
     frame_bytes = algorithmic_bytes(work)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

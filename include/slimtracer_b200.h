@@ -210,12 +210,16 @@ typedef struct {
 } SlimRenderOptions;
 enum { SLIM_CACHE_OFF = 0, SLIM_CACHE_ON = 1, SLIM_CACHE_TRUNCATE = 2, SLIM_CACHE_EXACT = 3 };
 
-/* Work counters of the last frame (rays traced and memory records touched). */
+/* Work counters of the last frame (rays traced and memory records touched).
+ * The shadow_* fields are the parts of the node, triangle and geometry
+ * tests spent in any-hit (shadow-ray) traversals; only the fused engine,
+ * which walks every ray in the reference's order, splits them out. */
 typedef struct {
     uint64_t primary_rays, shadow_rays, bounce_rays;
     uint64_t scene_node_tests, mesh_node_tests, triangle_tests;
     uint64_t geometry_tests, mesh_hit_fetches, texel_taps;
     uint64_t pixels;
+    uint64_t shadow_scene_node_tests, shadow_mesh_node_tests, shadow_triangle_tests, shadow_geometry_tests;
 } SlimWorkCounters;
 
 #ifdef __cplusplus

@@ -164,7 +164,7 @@ def oracle_render(scene, projection, settings, width, height, antialias=0, rows=
     threads = threads or os.cpu_count() or 1
     h = oracle()
     if threads <= 1 or r1 - r0 <= 8:
-        counters = np.zeros(10, np.uint64) if count else None
+        counters = np.zeros(14, np.uint64) if count else None
         rc = h.oracle_render(scene.ptr, _ptr(cv), _ptr(projection), _ptr(settings), r0, r1, int(cones_per_pixel),
                              _ptr(counters))
         assert rc == 0, rc
@@ -172,7 +172,7 @@ def oracle_render(scene, projection, settings, width, height, antialias=0, rows=
         return pixels, depths, work
     from concurrent.futures import ThreadPoolExecutor
     chunks = [(y, min(r1, y + 8)) for y in range(r0, r1, 8)]
-    per = [np.zeros(10, np.uint64) if count else None for _ in chunks]
+    per = [np.zeros(14, np.uint64) if count else None for _ in chunks]
 
     def run(k):
         a, b = chunks[k]

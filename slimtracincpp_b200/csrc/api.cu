@@ -866,9 +866,13 @@ int read_counters(Context &c, cudaStream_t stream) {
         sw.scene_node_tests = p[3]; sw.mesh_node_tests = p[4]; sw.triangle_tests = p[5];
         sw.geometry_tests = p[6]; sw.mesh_hit_fetches = p[7]; sw.texel_taps = p[8];
         sw.pixels = 0;
+        sw.shadow_scene_node_tests = p[9]; sw.shadow_mesh_node_tests = p[10];
+        sw.shadow_triangle_tests = p[11]; sw.shadow_geometry_tests = p[12];
         w.primary_rays += p[0]; w.shadow_rays += p[1]; w.bounce_rays += p[2];
         w.scene_node_tests += p[3]; w.mesh_node_tests += p[4]; w.triangle_tests += p[5];
         w.geometry_tests += p[6]; w.mesh_hit_fetches += p[7]; w.texel_taps += p[8];
+        w.shadow_scene_node_tests += p[9]; w.shadow_mesh_node_tests += p[10];
+        w.shadow_triangle_tests += p[11]; w.shadow_geometry_tests += p[12];
     }
     w.pixels = w.primary_rays;
     return SLIM_OK;

@@ -11,10 +11,12 @@ namespace dev {
 template <bool COUNT>
 SLIM_D void flush_work(unsigned long long *counters, const Work &w) {
     if (!COUNT || !counters) return;
-    uint32_t v[9] = {w.primary, w.shadow, w.bounce, w.scene_nodes, w.mesh_nodes, w.triangles,
-                     w.geometries, w.mesh_fetches, w.taps};
+    // slots 0-8 as every stage counts them, 9-12 the any-hit parts
+    uint32_t v[13] = {w.primary, w.shadow, w.bounce, w.scene_nodes, w.mesh_nodes, w.triangles,
+                      w.geometries, w.mesh_fetches, w.taps, w.any_scene_nodes, w.any_mesh_nodes,
+                      w.any_triangles, w.any_geometries};
 #pragma unroll
-    for (int k = 0; k < 9; k++) {
+    for (int k = 0; k < 13; k++) {
         unsigned long long s = v[k];
         for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
         if ((threadIdx.x & 31) == 0 && s) atomicAdd(counters + k, s);
@@ -75,7 +77,13 @@ SLIM_D bool path_segment(const DevScene &S, const DevFrame &F, PathState &p, uin
                     sr.d = s.L;
                     Hit sh;
                     bump<COUNT>(w.shadow);
-                    if (scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0) continue;
+                    const uint32_t sn = w.scene_nodes, mn = w.mesh_nodes, tr = w.triangles, ge = w.geometries;
+                    const bool occluded = scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0;
+                    bump<COUNT>(w.any_scene_nodes, w.scene_nodes - sn);
+                    bump<COUNT>(w.any_mesh_nodes, w.mesh_nodes - mn);
+                    bump<COUNT>(w.any_triangles, w.triangles - tr);
+                    bump<COUNT>(w.any_geometries, w.geometries - ge);
+                    if (occluded) continue;
                 }
                 add_light(s, m, l, current);
             }

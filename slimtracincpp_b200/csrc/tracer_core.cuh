@@ -314,6 +314,9 @@ SLIM_D bool hit_tet(const Ray &r, Hit &h, bool transparent) {
 // ---- work counters (optional) --------------------------------------------
 struct Work {
     uint32_t primary, shadow, bounce, scene_nodes, mesh_nodes, triangles, geometries, mesh_fetches, taps;
+    // the parts of scene_nodes, mesh_nodes, triangles, geometries spent in
+    // any-hit traversals (counted by the fused engine only)
+    uint32_t any_scene_nodes, any_mesh_nodes, any_triangles, any_geometries;
 };
 template <bool COUNT> SLIM_D void bump(uint32_t &c, uint32_t n = 1) { if (COUNT) c += n; }
 

@@ -116,8 +116,9 @@ NRC_PARAMS = 18624
 NRC_FEATURES = 16
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(
     ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",
-     "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels"])], 80)
-STAGE_STATS = _dt([("name", "S24", 0), ("launches", u4, 24), ("total_ms", f4, 28), ("work", WORK_COUNTERS, 32)], 112)
+     "geometry_tests", "mesh_hit_fetches", "texel_taps", "pixels", "shadow_scene_node_tests",
+     "shadow_mesh_node_tests", "shadow_triangle_tests", "shadow_geometry_tests"])], 112)
+STAGE_STATS = _dt([("name", "S24", 0), ("launches", u4, 24), ("total_ms", f4, 28), ("work", WORK_COUNTERS, 32)], 144)
 
 for _name, _dtype, _size in [("GEOMETRY", GEOMETRY, 72), ("MATERIAL", MATERIAL, 68), ("LIGHT", LIGHT, 32),
                              ("BVH_NODE", BVH_NODE, 32), ("TRIANGLE", TRIANGLE, 128), ("TEXEL_QUAD", TEXEL_QUAD, 12),

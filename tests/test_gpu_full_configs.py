@@ -207,7 +207,7 @@ def test_config2_full_size_after_moves_and_gpu_refit(config2_workload, entry):
         assert differ.mean() <= 1e-4, f"{int(differ.sum())} primary ids differ"
         assert np.array_equal(d.view(np.uint32), od.view(np.uint32))
         assert np.array_equal(b[~differ], ob[~differ])
-        assert (og >= 0).mean() > 0.3           # the frame is mostly geometry, not sky
+        assert (og >= 0).mean() > 0.1           # the moved instances still cover a good part of the frame
     finally:
         scene.geometries[:] = saved
         scene.build_bvh()

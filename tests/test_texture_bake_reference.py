@@ -91,8 +91,19 @@ def test_host_baker_matches_reference_converter(name, tmp_path):
     assert checked >= 8
 
 
+# Cube strips of these heights.  The converter writes two texel quads past
+# the end of the main strip's quad array when it fills the seams
+# (bmp2texture.cpp:99,126 size a quad row as (w + 1) * 4 where the strip has
+# 4w + 1 quads), a heap overflow whose effect depends on the allocator: with
+# glibc at h = 16 it lands on texel 10 of the top face's texel array, which
+# the converter has already allocated, and changes that texel's four
+# corners.  The bakers here keep their writes in bounds, so heights whose
+# overflow reaches a live array are not comparable; 4, 8, 12, 24 and 32 are.
+CUBE_HEIGHTS = [4, 8, 12, 24, 32]
+
+
 @needs_tool
-@pytest.mark.parametrize("h", [4, 8, 32])
+@pytest.mark.parametrize("h", CUBE_HEIGHTS)
 def test_cube_strip_matches_reference_converter(h, tmp_path):
     rng = np.random.default_rng(h)
     img = rng.integers(0, 256, (h, 6 * h, 3), dtype=np.uint8)
@@ -113,6 +124,7 @@ def test_gpu_baker_matches_reference_converter(name, tmp_path):
         ref = reference_texture(tmp_path, img, switches)
         got = ours(img, flags | (L.IMAGE_ALPHA if ch == 4 else 0), on_gpu=True, tmp_path=tmp_path)
         assert got == ref, (name, w, h, ch)
-    cube = rng.integers(0, 256, (16, 96, 3), dtype=np.uint8)
-    assert ours(cube, L.IMAGE_CUBEMAP | L.IMAGE_LINEAR, on_gpu=True, tmp_path=tmp_path) == \
-        reference_texture(tmp_path, cube, ["-c", "-l"])
+    for h in (8, 32):
+        cube = rng.integers(0, 256, (h, 6 * h, 3), dtype=np.uint8)
+        assert ours(cube, L.IMAGE_CUBEMAP | L.IMAGE_LINEAR, on_gpu=True, tmp_path=tmp_path) == \
+            reference_texture(tmp_path, cube, ["-c", "-l"])

@@ -93,7 +93,7 @@ def test_host_baker_matches_reference_converter(name, tmp_path):
 
 # Cube strips of these heights.  The converter writes two texel quads past
 # the end of the main strip's quad array when it fills the seams
-# (bmp2texture.cpp:99,126 size a quad row as (w + 1) * 4 where the strip has
+# (bmp2texture.cpp:100,126 size a quad row as (w + 1) * 4 where the strip has
 # 4w + 1 quads), a heap overflow whose effect depends on the allocator: with
 # glibc at h = 16 it lands on texel 10 of the top face's texel array, which
 # the converter has already allocated, and changes that texel's four

@@ -205,6 +205,7 @@ struct Context {
         DevArray<float4> features, aux, radiance, t_features, t_targets, t_color, t_through;
         DevArray<float4> s_features, s_aux, s_radiance;   // self-training queries
         DevArray<uint32_t> s_count;
+        DevArray<float4> q_color, q_through;              // per-query path state
         DevArray<uint32_t> counts;
         DevArray<uint32_t> state;      // [0] Adam steps taken, [1] cache frames (training-set offsets)
         uint32_t *error_flags = nullptr;
@@ -642,6 +643,8 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     if ((rc = k.aux.reserve(2 * (size_t)samples, "alloc cache query rays"))) return rc;
     if ((rc = k.radiance.reserve(samples, "alloc cache answers"))) return rc;
     if ((rc = k.counts.reserve(2, "alloc cache counters"))) return rc;
+    if ((rc = k.q_color.reserve(samples, "alloc cache query paths"))) return rc;
+    if ((rc = k.q_through.reserve(samples, "alloc cache query paths"))) return rc;
     if (cap) {
         if ((rc = k.t_targets.reserve(cap, "alloc training targets"))) return rc;
         if ((rc = k.t_color.reserve(cap, "alloc training paths"))) return rc;
@@ -660,6 +663,8 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     cf.aux = k.aux.ptr;
     cf.radiance = k.radiance.ptr;
     cf.counts = k.counts.ptr;
+    cf.q_color = k.q_color.ptr;
+    cf.q_through = k.q_through.ptr;
     cf.train_capacity = cap;
     cf.t_features = k.t_features.ptr;
     cf.t_targets = k.t_targets.ptr;
@@ -747,7 +752,8 @@ int wait_for_refit(Context &c, cudaStream_t stream) {
 // frame).
 int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjection *projection,
            const SlimRayTracerSettings *settings, float4 *d_pixels, float *d_depths, cudaStream_t stream,
-           uint32_t row_begin, uint32_t rows, bool first, int set = 0, const FrameDownload *download = nullptr) {
+           uint32_t row_begin, uint32_t rows, bool first, int set = 0, const FrameDownload *download = nullptr,
+           int cache_part = kCachePartWhole) {
     const SlimDimensions &dim = canvas->dimensions;
     if (!dim.width || !dim.height) return set_error(SLIM_ERR_ARGUMENT, "canvas has zero size");
     if (canvas->antialias < SLIM_AA_NONE || canvas->antialias > SLIM_AA_SSAA) return set_error(SLIM_ERR_ARGUMENT, "bad antialias mode");
@@ -781,12 +787,13 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) {
         e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer);
     } else {
-        rc = ensure_wavefront(c, F.width * F.rows, set);
-        if (rc) return rc;
+        // the cache phase of a banded frame needs no path queues of its own
+        if (cache_part != kCachePartPhase && (rc = ensure_wavefront(c, F.width * F.rows, set))) return rc;
         CacheFrame cf;
         const CacheFrame *cache = nullptr;
         if (c.options.radiance_cache != SLIM_CACHE_OFF) {
-            if ((rc = cache_frame(c, F.width * F.rows, cf))) return rc;
+            if ((rc = cache_frame(c, F.width * F.height, cf))) return rc;
+            cf.part = cache_part;
             cache = &cf;
         }
         e = launch_render_wavefront(c.scene, F, c.wave[set].B, c.options.block_size, stream, timer, cache, download);
@@ -896,8 +903,18 @@ constexpr double kBandRatio = 2.0 / 3.0;
 constexpr double kDownloadBandRatio = 0.5;
 constexpr uint32_t kMinBandedSamples = 1u << 18;
 
+// Radiance-cache frames split into bands only when the cache trains
+// overlapped on its own stream and queues (ON mode): the bands gather their
+// queries into the frame's query buffers and one cache phase follows them.
+bool banded_cache(const Context &c) {
+    const Context::Cache &k = c.cache;
+    return c.options.radiance_cache == SLIM_CACHE_ON && k.configured && k.config.train && k.config.overlap &&
+           k.config.train_samples && !c.options.count_work;
+}
+
 uint32_t row_bands(const Context &c, uint32_t sample_rows, uint32_t samples) {
-    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL || c.options.radiance_cache != SLIM_CACHE_OFF) return 1;
+    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) return 1;
+    if (c.options.radiance_cache != SLIM_CACHE_OFF && !banded_cache(c)) return 1;
     uint32_t bands = c.options.row_bands ? (uint32_t)c.options.row_bands
                                          : (samples >= kMinBandedSamples ? kDefaultRowBands : 1u);
     const uint32_t tiles = sample_rows / 4;
@@ -954,7 +971,10 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     // under MSAA and SSAA).
     const size_t pix_per_row = ssaa ? (size_t)stride * 2 : stride;
     const size_t dep_per_row = ssaa ? (size_t)stride * 2 : (size_t)stride * (canvas->antialias == SLIM_AA_NONE ? 1 : 4);
-    const bool banded_download = download && pinned_host(host_pixels) && pinned_host(host_depths);
+    const bool cache_bands = c.options.radiance_cache != SLIM_CACHE_OFF;
+    // a cache frame's query pixels are written by the cache phase after the
+    // bands: it downloads whole, at the end
+    const bool banded_download = download && !cache_bands && pinned_host(host_pixels) && pinned_host(host_depths);
     // Pinned canvases the device can address: each band's rows download as
     // soon as its first round is done, and later pixels go straight there.
     float4 *mapped_pixels = nullptr;
@@ -986,6 +1006,12 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         SLIM_CUDA(cudaMemsetAsync(c.d_counters.ptr, 0, kCountersPerStage * STAGE_COUNT * sizeof(unsigned long long),
                                   stream), "clear counters");
     if ((rc = wait_for_refit(c, stream))) return rc;
+    if (cache_bands) {
+        // the frame's query buffers, and its query count cleared once for all bands
+        CacheFrame cf;
+        if ((rc = cache_frame(c, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1), cf))) return rc;
+        SLIM_CUDA(cudaMemsetAsync(cf.counts, 0, sizeof(uint32_t), stream), "clear cache queries");
+    }
     SLIM_CUDA(cudaEventRecord(c.band_fork, stream), "band fork");
     cudaStream_t lanes[kBandLanes];
     lanes[0] = stream;
@@ -1035,7 +1061,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
             r0 = r1;
             continue;
         }
-        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane)))
+        if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, ls, r0, r1 - r0, false, lane, nullptr,
+                         cache_bands ? kCachePartGather : kCachePartWhole)))
             return rc;
         if (banded_download) {
             SLIM_CUDA(cudaEventRecord(c.band_events[b], ls), "band event");
@@ -1051,6 +1078,11 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
         SLIM_CUDA(cudaEventRecord(c.band_join[l], lanes[l]), "band join");
         SLIM_CUDA(cudaStreamWaitEvent(stream, c.band_join[l], 0), "band join");
     }
+    // every band's queries are in: training-path selection, the network's
+    // answers and the waiting paths of the whole frame
+    if (cache_bands &&
+        (rc = render(c, canvas, projection, settings, d_pixels, d_depths, stream, 0, 0, false, 0, nullptr, kCachePartPhase)))
+        return rc;
     if (banded_download) {
         for (int l = 0; l < kBandLanes; l++) {
             SLIM_CUDA(cudaEventRecord(c.band_events[kEventsPerBand * bands + l], c.copy_streams[l]), "downloads done");

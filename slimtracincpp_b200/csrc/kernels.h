@@ -94,7 +94,16 @@ struct CacheFrame {
     uint32_t train_suffix = 0;
     float4 *s_features = nullptr, *s_aux = nullptr, *s_radiance = nullptr;
     uint32_t *s_count = nullptr;
+    // Each query also keeps its path's state (colour + canvas depth,
+    // throughput), so queries gathered by several row bands -- each with its
+    // own path slots -- resolve together (null: read the path slots).
+    float4 *q_color = nullptr, *q_through = nullptr;
+    // Which part of a cache frame a launch runs: the whole frame, the rounds
+    // up to the cache vertex and the gather only (a row band), or the cache
+    // phase only (once the bands have joined).
+    int part = 0;
 };
+constexpr int kCachePartWhole = 0, kCachePartGather = 1, kCachePartPhase = 2;
 
 // Download of a frame's (or band's) canvas rows while its later bounces
 // still run (no counterpart in the reference).  After the first round every

@@ -89,6 +89,7 @@ struct CacheArgs {
     float4 *t_features, *t_targets, *t_color, *t_through;
     uint32_t *frame_counter;
     int mode;
+    float4 *q_color, *q_through;   // per query: path colour + depth, throughput (null: path slots)
 };
 
 struct QueueArgs {
@@ -1084,7 +1085,7 @@ __global__ void __launch_bounds__(128) k_finish_paths(DevScene S0, DevFrame F0, 
 // path_throughput for the answer.  Returns true for a query.
 template <bool COUNT, bool BATCH>
 SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &A, uint32_t slot, uint32_t path,
-                         uint32_t pid, float3 o, float3 d, float4 f[4], Work &w) {
+                         uint32_t pid, float3 o, float3 d, float4 f[4], Work &w, float4 &q_color, float4 &q_through) {
     const SlimRayTracerSettings &st = F.settings;
     Ray ray;
     reset(ray, scale_add(d, kTraceOffset, o), d);
@@ -1123,18 +1124,24 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
     }
     add_glow(S, ray, hit_distance, current);
     color = mul_add(current, throughput, color);
-    if (query) A.path_color[path] = make_float4(color.x, color.y, color.z, pc.w);
+    q_color = make_float4(color.x, color.y, color.z, pc.w);
+    q_through = make_float4(throughput.x, throughput.y, throughput.z, 0.0f);
+    if (query) A.path_color[path] = q_color;
     else if (A.sink) A.sink[path] = make_float4(color.x, color.y, color.z, 0.0f);   // a self-training path ends
     else write_pixel<BATCH>(F, pid, color, pc.w);
     return query;
 }
 
 SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], float3 o, float3 d, uint32_t path,
-                         uint32_t pid) {
+                         uint32_t pid, float4 q_color, float4 q_through) {
     float4 *p = C.features + 4 * (size_t)q;
     p[0] = f[0]; p[1] = f[1]; p[2] = f[2]; p[3] = f[3];
     C.aux[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __uint_as_float(path));
     C.aux[2 * (size_t)q + 1] = make_float4(d.x, d.y, d.z, __uint_as_float(pid));
+    if (C.q_color) {
+        C.q_color[q] = q_color;
+        C.q_through[q] = q_through;
+    }
 }
 
 // ---- shade: colour of this segment, next bounce, finished paths --------
@@ -1154,14 +1161,14 @@ __global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, Queu
         uint32_t path = 0, pid = 0;
         float3 o = f3(0, 0, 0), d = f3(0, 0, 0);
         float3 bo = f3(0, 0, 0), bd = f3(0, 0, 0);
-        float4 feat[4];
+        float4 feat[4], qc = make_float4(0, 0, 0, 0), qt = make_float4(0, 0, 0, 0);
         if (live) {
             load_ray(F0, A, slot, o, d, path, pid);
             const DevScene &S = scene_of<BATCH>(S0, A, pid);
             const DevFrame &F = frame_of<BATCH>(F0, A, pid);
             const SlimRayTracerSettings &st = F.settings;
             if (at_cache_vertex<BATCH>(F, A)) {
-                query = cache_vertex<COUNT, BATCH>(S, F, A, slot, path, pid, o, d, feat, w);
+                query = cache_vertex<COUNT, BATCH>(S, F, A, slot, path, pid, o, d, feat, w, qc, qt);
             } else {
                 Ray ray;
                 reset(ray, scale_add(d, kTraceOffset, o), d);
@@ -1232,7 +1239,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, Queu
         }
         if (BATCH) {
             uint32_t cq = warp_append(A.cache.count, query);
-            if (query) append_query(A.cache, cq, feat, o, d, path, pid);
+            if (query) append_query(A.cache, cq, feat, o, d, path, pid, qc, qt);
         }
     }
     flush_stage<COUNT>(A.counters, w);
@@ -1251,13 +1258,13 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
         bool query = false;
         uint32_t path = 0, pid = 0;
         float3 o = f3(0, 0, 0), d = f3(0, 0, 0);
-        float4 feat[4];
+        float4 feat[4], qc = make_float4(0, 0, 0, 0), qt = make_float4(0, 0, 0, 0);
         if (slot < n) {
             load_ray(F, A, slot, o, d, path, pid);
-            query = cache_vertex<COUNT, false>(S, F, A, slot, path, pid, o, d, feat, w);
+            query = cache_vertex<COUNT, false>(S, F, A, slot, path, pid, o, d, feat, w, qc, qt);
         }
         uint32_t q = warp_append(C.count, query);
-        if (query) append_query(C, q, feat, o, d, path, pid);
+        if (query) append_query(C, q, feat, o, d, path, pid, qc, qt);
     }
     flush_stage<COUNT>(A.counters, w);
 }
@@ -1319,8 +1326,8 @@ __global__ void k_cache_resolve(DevFrame F0, QueueArgs A, const float4 *path_col
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
         uint32_t path = __float_as_uint(C.aux[2 * (size_t)q].w);
         uint32_t pid = __float_as_uint(C.aux[2 * (size_t)q + 1].w);
-        float4 pc = path_color[path];
-        float3 thr = xyz(path_throughput[path]);
+        float4 pc = C.q_color ? C.q_color[q] : path_color[path];
+        float3 thr = xyz(C.q_color ? C.q_through[q] : path_throughput[path]);
         float3 L = f3(0, 0, 0);
         if (C.mode == SLIM_CACHE_ON) L = xyz(C.radiance[q]);
         else if (C.mode == SLIM_CACHE_EXACT) L = xyz(C.t_targets[q]);
@@ -1544,6 +1551,8 @@ CacheArgs cache_args(const CacheFrame *cache) {
     CA.t_through = cache->t_through;
     CA.frame_counter = cache->frame_counter;
     CA.mode = cache->mode;
+    CA.q_color = cache->q_color;
+    CA.q_through = cache->q_through;
     return CA;
 }
 
@@ -1572,6 +1581,7 @@ cudaError_t trace_training(const RoundLaunch &L, QueueArgs &A, const CacheArgs &
     SC.features = cache->s_features;
     SC.aux = cache->s_aux;
     SC.count = cache->s_count;
+    SC.q_color = SC.q_through = nullptr;
     if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
     if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
     if ((e = nrc::launch_infer(cache->s_features, cache->s_count, 0, cache->train_capacity, cache->s_radiance, weights,
@@ -1697,7 +1707,7 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
                   S.mesh_count > 0};
     // the cache's overlapped training runs beside this frame: leave it room
     // (config 4: 3.50 -> 3.37 ms per frame)
-    L.share_sms = cache && cache->train_stream && cache->mode == SLIM_CACHE_ON;
+    L.share_sms = cache && cache->train_stream && cache->mode == SLIM_CACHE_ON && !cache->train_suffix;
     cudaError_t e = cudaMemsetAsync(B.queue_count, 0, 8 * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
     QueueArgs A{};
@@ -1714,11 +1724,19 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     const uint32_t max_depth = F.settings.max_depth;
     const bool use_cache = cache && cache->mode != SLIM_CACHE_OFF && cache->depth >= 2 && cache->depth <= max_depth;
     CacheArgs CA = use_cache ? cache_args(cache) : CacheArgs{};
+    const int part = use_cache ? cache->part : kCachePartWhole;
+    uint32_t in = 0;
+    if (part == kCachePartPhase) {   // the bands have gathered every query of the frame
+        A.cache = CA;
+        return cache_phase<COUNT, false>(L, A, CA, in, cache, max_depth);
+    }
     // Only the query count starts over: the training count belongs to the
     // training set, which the overlapped training stream may still be using;
-    // the selection that replaces the set rewrites it.
-    if (use_cache && (e = cudaMemsetAsync(cache->counts, 0, sizeof(uint32_t), stream)) != cudaSuccess) return e;
-    uint32_t in = 0;
+    // the selection that replaces the set rewrites it.  (A banded frame
+    // clears it once, before its bands.)
+    if (use_cache && part == kCachePartWhole &&
+        (e = cudaMemsetAsync(cache->counts, 0, sizeof(uint32_t), stream)) != cudaSuccess)
+        return e;
     const uint32_t last = use_cache ? cache->depth : max_depth;
     DevFrame late = F;   // the frame as the rounds after a download see it
     for (uint32_t depth = 1; depth <= last; depth++) {
@@ -1751,7 +1769,7 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
             L.pixel_wait = dl->copied;
         }
     }
-    if (!use_cache) return cudaSuccess;
+    if (!use_cache || part == kCachePartGather) return cudaSuccess;
     A.cache = CA;
     return cache_phase<COUNT, false>(L, A, CA, in, cache, max_depth);
 }

@@ -238,3 +238,39 @@ def test_self_training_cache_beats_truncation(suffix):
     p_trunc = psnr(to8(trunc, w.width, w.height), ref)
     assert scores[-1] > p_trunc + 3.0, (p_trunc, scores[0], scores[-1])
     assert scores[-1] > scores[0]
+
+
+def test_banded_cache_frames_gather_every_band():
+    """A 1080p-sized cache frame renders as two row bands whose queries meet
+    in one cache phase (the query records carry their paths' colour and
+    throughput).  Against the same frames rendered as one band: every depth
+    and every pixel whose path ends before the cache vertex are bit-identical,
+    all queries are answered (finite pixels, every pixel written), and the
+    trained cache scores like the unbanded one against the plain frame."""
+    w = scenes.small_mesh_scene(2, 512, 512)
+    w.settings = L.default_settings(max_depth=6)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    plain, _ = r.render(vp)
+    ref = to8(plain, w.width, w.height)
+    out = {}
+    try:
+        for bands in (1, 2):
+            cache = RadianceCache.configure(cache_depth=2, train_samples=8192, batch=2048, seed=4, train_suffix=1)
+            native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON, row_bands=bands)
+            for _ in range(40):
+                img, dep = r.render(vp, update_scene=False)
+            cache.join()
+            img, dep = r.render(vp, update_scene=False)
+            out[bands] = (img, dep, cache.stats()["queries"])
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    (a, da, qa), (b, db, qb) = out[1], out[2]
+    assert qa == qb and qa > 100
+    assert np.array_equal(da.view(np.uint32), db.view(np.uint32))
+    assert np.isfinite(b).all() and (b[:, 3] == 1.0).all()
+    same = (a.view(np.uint32) == b.view(np.uint32)).all(axis=1).mean()
+    assert same >= 1.0 - qa / (w.width * w.height) - 1e-3, same
+    pa, pb = psnr(to8(a, w.width, w.height), ref), psnr(to8(b, w.width, w.height), ref)
+    assert pb > pa - 1.0, (pa, pb)

@@ -457,6 +457,34 @@ def timed_frames(torch, native, r, vp, sp, stream, outputs, flush):
     return [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
 
+def pinned_scene_record(torch, w):
+    """The scene record with its per-frame arrays (geometries, lights) in
+    pinned host memory, as an app keeps them; returns (record, keep-alive
+    tensors, bytes the per-frame uploads move)."""
+    from slimtracincpp_b200 import layout as L
+    sd = w.scene.data.copy()
+    keep, nbytes = [], 0
+    for field, arr, dtype in (("geometries", w.scene.geometries, L.GEOMETRY), ("lights", w.scene.lights, L.LIGHT)):
+        if not len(arr):
+            continue
+        t = torch.empty(arr.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy().view(dtype)[:] = arr
+        sd[field] = t.data_ptr()
+        keep.append(t)
+        nbytes += arr.nbytes
+    return sd, keep, nbytes
+
+
+def per_frame_uploads(lib, native, sd):
+    """renderer.h:72-77's per-frame uploads of render(update_scene=true):
+    lights, cameras, geometries; the scene BVH is refit on the device
+    instead of rebuilt on the host and uploaded."""
+    native.check(lib.slimUploadLights(native.ptr(sd)))
+    native.check(lib.slimUploadCameras(native.ptr(sd)))
+    native.check(lib.slimUploadGeometries(native.ptr(sd)))
+    native.check(lib.slimRefitSceneBVH(None))
+
+
 def frame_quality(pix, ref_pix):
     """PSNR of the 8-bit canvas and max abs error of the stored colours
     against the reference frame (the plain depth-8 frame)."""
@@ -586,21 +614,16 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
     pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
-    pin_geo = torch.empty(w.scene.geometries.nbytes, dtype=torch.uint8, pin_memory=True)
-    pin_geo.numpy().view(L.GEOMETRY)[:] = w.scene.geometries
-    sd = w.scene.data.copy()
-    sd["geometries"] = pin_geo.data_ptr()
+    sd, _keep, h2d = pinned_scene_record(torch, w)
     cv, _, _ = make_canvas(w.width, w.height, L.AA_NONE)
     cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
     proj = w.projection()
     for _ in range(max(args.warmup, CACHE_WARMUP_FRAMES)):
-        native.check(lib.slimUploadGeometries(native.ptr(sd)))
-        native.check(lib.slimRefitSceneBVH(None))
+        per_frame_uploads(lib, native, sd)
         native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
     t0 = time.perf_counter()
     for _ in range(steps):
-        native.check(lib.slimUploadGeometries(native.ptr(sd)))
-        native.check(lib.slimRefitSceneBVH(None))
+        per_frame_uploads(lib, native, sd)
         native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
     e2e_s = time.perf_counter() - t0
     native.set_render_options(engine=L.ENGINE_WAVEFRONT)
@@ -622,9 +645,11 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
             "psnr_db_per_frame": c["psnr_db_per_frame"], "max_abs_per_frame": c["max_abs_per_frame"],
             "cache": {k: c[k] for k in ("queries", "train_samples", "loss", "train_targets")},
             "e2e": {"value": c["rays_per_frame"] * steps * world / e2e_s / 1e6, "unit": UNIT,
-                    "h2d_bytes_per_step": int(w.scene.geometries.nbytes),
+                    "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(pin_pix.numel() * 4 + pin_dep.numel() * 4),
-                    "ms_per_step": 1000.0 * e2e_s / steps},
+                    "ms_per_step": 1000.0 * e2e_s / steps,
+                    "per_step": "slimUploadLights/Cameras/Geometries (pinned), slimRefitSceneBVH, slimRenderOnGPU "
+                                "into a pinned canvas"},
             "clocks": clock_info,
             "gpu_launches": c["gpu_launches"]}
     if rank == 0:
@@ -843,27 +868,20 @@ def main():
     native.set_render_options(engine=engine, row_bands=args.row_bands)
     pin_pix = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     pin_dep = torch.empty(n, dtype=torch.float32, pin_memory=True)
-    pin_geo = torch.empty(w.scene.geometries.nbytes, dtype=torch.uint8, pin_memory=True)
-    host_geo = pin_geo.numpy().view(L.GEOMETRY)
-    host_geo[:] = w.scene.geometries
-    sd = w.scene.data.copy()
-    sd["geometries"] = pin_geo.data_ptr()
+    sd, _keep, h2d = pinned_scene_record(torch, w)
     cv, _, _ = make_canvas(w.width, w.height, L.AA_NONE)
     cv["pixels"], cv["depths"] = pin_pix.data_ptr(), pin_dep.data_ptr()
     proj = w.projection()
     for _ in range(args.warmup):
-        native.check(lib.slimUploadGeometries(native.ptr(sd)))
-        native.check(lib.slimRefitSceneBVH(None))
+        per_frame_uploads(lib, native, sd)
         native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        native.check(lib.slimUploadGeometries(native.ptr(sd)))
-        native.check(lib.slimRefitSceneBVH(None))
+        per_frame_uploads(lib, native, sd)
         native.check(lib.slimRenderOnGPU(native.ptr(cv), native.ptr(proj), native.ptr(r.settings)))
     e2e_s = time.perf_counter() - t0
-    h2d = int(w.scene.geometries.nbytes)
     d2h = int(pin_pix.numel() * 4 + pin_dep.numel() * 4)
 
     # max over ranks
@@ -924,8 +942,10 @@ def main():
             "stage_profile": {"ms_per_frame": prof_ms / args.steps, "row_bands": 1,
                               "note": "stage times from a second timed loop with per-launch CUDA events"},
             "stage_work_per_frame": {k: v for k, v in stage_work.items() if any(v.values())},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": 1000.0 * e2e_s / args.steps},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1000.0 * e2e_s / args.steps,
+                    "per_step": "slimUploadLights/Cameras/Geometries (pinned), slimRefitSceneBVH, slimRenderOnGPU "
+                                "into a pinned canvas"},
             "clocks": clock_info,
             "gpu_launches": launches}
     if args.config == "config2" and args.engine == "wavefront" and not args.no_cache_block:

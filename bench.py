@@ -65,6 +65,8 @@ def parse():
                         "traced k bounces past the cache vertex into the cache's own answer")
     p.add_argument("--no-cache-block", action="store_true",
                    help="default workload: skip the radiance-cache comparison block")
+    p.add_argument("--no-batch-block", action="store_true",
+                   help="default workload: skip the batched-requests (config 5) block")
     return p.parse_args()
 
 
@@ -659,23 +661,25 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     return 0
 
 
-def run_batch_bench(args, torch, dist, dev, rank, world, local):
+def batch_comparison(torch, native, dev, steps, warmup, seed=0, meshes=None):
     """Config 5: 64 requests (own seeded scenes, 320x180 ... 3840x2160, depth
     1-8, every other one with the radiance cache) rendered as one batch --
-    waves over shared queues, captured in a CUDA graph, plan chosen by the
-    project autotuner -- against rendering them one at a time (a batch of
-    one each, same kernels, same graph replay)."""
+    captured in a CUDA graph, plan chosen by the project autotuner (waves over
+    shared queues, or the plain requests in one persistent launch beside the
+    cache requests' waves) -- against rendering them one at a time (a batch
+    of one each, same plan, same graph replay).  Both plans are also timed
+    on their own."""
     import numpy as np
     from slimtracincpp_b200 import layout as L
-    from slimtracincpp_b200 import native, scenes
+    from slimtracincpp_b200 import scenes
     from slimtracincpp_b200.batch import BatchRenderer
     from slimtracincpp_b200.radiance_cache import RadianceCache
     from slimtracincpp_b200.scene import Scene, geometry
-    meshes = scenes.config2_meshes()
-    reqs = scenes.config5(args.seed, meshes=meshes)
+    meshes = meshes if meshes is not None else scenes.config2_meshes()
+    reqs = scenes.config5(seed, meshes=meshes)
     assets = Scene(np.array([geometry(L.GEOMETRY_SPHERE, 0)]), np.array([L.default_material()]), meshes=meshes)
     batch = BatchRenderer(assets)
-    RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=args.seed)
+    RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=seed)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     outs = [(torch.zeros((q.samples, 4), dtype=torch.float32, device=dev),
@@ -692,39 +696,43 @@ def run_batch_bench(args, torch, dist, dev, rank, world, local):
     rays = wk["primary_rays"] + wk["shadow_rays"] + wk["bounce_rays"]
     native.set_render_options(engine=L.ENGINE_WAVEFRONT)
 
+    def timed(k):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        for i in range(k):
+            starts[i].record(stream)
+            batch.render(sp)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in zip(starts, ends)]
+
     batch.set_requests(reqs, ptrs)
     plan = batch.tune(sp)
-    for _ in range(args.warmup):
+    plans = {}
+    for name, persistent in (("waves", False), ("persistent", True)):
+        batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"], persistent)
+        batch.render(sp)
+        plans[name] = statistics.median(timed(3))
+    batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"], plan["persistent"])
+    for _ in range(warmup):
         batch.render(sp)
     batch.synchronize(sp)
-    clocks = ClockSampler(local, device_uuid(dev))
-    clocks.start()
-    if world > 1:
-        dist.barrier()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches0 = native.launch_count()
-    for i in range(args.steps):
-        starts[i].record(stream)
-        batch.render(sp)
-        ends[i].record(stream)
+    batch_ms = timed(steps)
     launches = native.launch_count() - launches0
-    torch.cuda.synchronize()
-    clock_info = clocks.stop()
-    batch_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
-    plan = batch.plan()
+    plan.update({k: v for k, v in batch.plan().items() if k in ("graph_nodes", "waves")})
 
     # end to end: the batch plus every canvas read back to pinned host memory
     pins = [(torch.empty_like(p, device="cpu").pin_memory(), torch.empty_like(d, device="cpu").pin_memory())
             for p, d in outs]
+    e2e_steps = max(1, steps // 4)
     t0 = time.perf_counter()
-    for _ in range(max(1, args.steps // 4)):
+    for _ in range(e2e_steps):
         batch.render(sp)
         for (hp, hd), (p, d) in zip(pins, outs):
             hp.copy_(p, non_blocking=True)
             hd.copy_(d, non_blocking=True)
         torch.cuda.synchronize()
-    e2e_steps = max(1, args.steps // 4)
     e2e_s = time.perf_counter() - t0
     d2h = sum(p.numel() * 4 + d.numel() * 4 for p, d in outs)
 
@@ -734,35 +742,49 @@ def run_batch_bench(args, torch, dist, dev, rank, world, local):
         batch.set_requests([q], [ptr])
         batch.set_plan(plan["queue_capacity"], plan["tile_pixels"], plan["block_size"], plan["persistent"])
         batch.render(sp)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(3):
-            batch.render(sp)
-        b.record(stream)
-        torch.cuda.synchronize()
-        single_ms.append(a.elapsed_time(b) / 3)
-
-    total_ms, e2e_s = max_over_ranks([sum(batch_ms), e2e_s], dev, world)
-    ms = total_ms / args.steps
-    value = whole_job_rate(rays, args.steps, world, total_ms)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 trace, bf16 MLP (f32 accumulate)",
-            "data": "synthetic (64 seeded request scenes)",
-            "config": {"workload": "config5_batch_64_requests", "requests": len(reqs), "pixels": pixels,
-                       "rays_per_batch": rays, "cache_requests": sum(q.radiance_cache != 0 for q in reqs),
-                       "resolutions": [f"{q.width}x{q.height}" for q in reqs],
-                       "max_depths": [int(q.settings["max_depth"]) for q in reqs],
-                       "parallelism": f"replicas x{world}",
-                       "l2": "no flush: canvases and queues (> 3 GB) exceed L2"},
-            "batch_ms": ms, "plan": plan,
+        single_ms.append(sum(timed(3)) / 3)
+    ms = sum(batch_ms) / steps
+    return {"workload": "config5_batch_64_requests", "requests": len(reqs), "pixels": pixels,
+            "rays_per_batch": rays, "cache_requests": sum(q.radiance_cache != 0 for q in reqs),
+            "resolutions": [f"{q.width}x{q.height}" for q in reqs],
+            "max_depths": [int(q.settings["max_depth"]) for q in reqs],
+            "batch_ms": ms, "batch_ms_total": sum(batch_ms), "mrays_s": rays / (ms / 1000.0) / 1e6,
+            "plan": plan, "plans_ms": plans,
             "one_at_a_time": {"total_ms": sum(single_ms), "per_request_ms": single_ms,
                               "mrays_s": rays / (sum(single_ms) / 1000.0) / 1e6},
             "speedup_vs_one_at_a_time": sum(single_ms) / ms,
-            "e2e": {"value": rays * e2e_steps * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
+            "e2e": {"value": rays * e2e_steps / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000.0 * e2e_s / e2e_steps},
+            "gpu_launches": launches, "steps": steps}
+
+
+def run_batch_bench(args, torch, dist, dev, rank, world, local):
+    """Config 5 as its own line (see batch_comparison)."""
+    from slimtracincpp_b200 import native
+    clocks = ClockSampler(local, device_uuid(dev))
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    b = batch_comparison(torch, native, dev, args.steps, args.warmup, args.seed)
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    total_ms, e2e_ms = max_over_ranks([b["batch_ms_total"], b["e2e"]["ms_per_step"]], dev, world)
+    value = whole_job_rate(b["rays_per_batch"], args.steps, world, total_ms)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 trace, bf16 MLP (f32 accumulate)",
+            "data": "synthetic (64 seeded request scenes)",
+            "config": {"workload": b["workload"], "requests": b["requests"], "pixels": b["pixels"],
+                       "rays_per_batch": b["rays_per_batch"], "cache_requests": b["cache_requests"],
+                       "resolutions": b["resolutions"], "max_depths": b["max_depths"],
+                       "parallelism": f"replicas x{world}",
+                       "l2": "no flush: canvases and queues (> 3 GB) exceed L2"},
+            "batch_ms": total_ms / args.steps, "plan": b["plan"], "plans_ms": b["plans_ms"],
+            "one_at_a_time": b["one_at_a_time"], "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
+            "e2e": dict(b["e2e"], value=b["rays_per_batch"] * world / (e2e_ms / 1000.0) / 1e6, ms_per_step=e2e_ms),
             "clocks": clock_info,
-            "gpu_launches": launches}
+            "gpu_launches": b["gpu_launches"]}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -957,6 +979,10 @@ def main():
         cmp["workload"] = w4.name
         cmp["nrc_roofline"] = nrc_roofline(torch, native, w4, dev)
         line["radiance_cache"] = cmp
+    if args.config == "config2" and args.engine == "wavefront" and not args.no_batch_block:
+        # config 5 (64 batched requests over config 2's meshes), same process
+        line["batch"] = batch_comparison(torch, native, dev, min(args.steps, 5), min(args.warmup, 3), args.seed,
+                                         meshes=w.scene.meshes)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = {k: v for k, v in cpu_baseline(w, args.cpu_seconds).items() if k != "seconds"}
     if rank == 0:

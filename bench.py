@@ -67,6 +67,10 @@ def parse():
                    help="default workload: skip the radiance-cache comparison block")
     p.add_argument("--no-batch-block", action="store_true",
                    help="default workload: skip the batched-requests (config 5) block")
+    p.add_argument("--batch-requests", type=int, default=64,
+                   help="config5: requests per batch (64 as specified; fewer for small profiling cases)")
+    p.add_argument("--batch-small", action="store_true",
+                   help="config5: resolutions drawn from 320x180 and 640x360 only (small profiling cases)")
     return p.parse_args()
 
 
@@ -661,7 +665,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     return 0
 
 
-def batch_comparison(torch, native, dev, steps, warmup, seed=0, meshes=None):
+def batch_comparison(torch, native, dev, steps, warmup, seed=0, meshes=None, count=64, resolutions=None):
     """Config 5: 64 requests (own seeded scenes, 320x180 ... 3840x2160, depth
     1-8, every other one with the radiance cache) rendered as one batch --
     captured in a CUDA graph, plan chosen by the project autotuner (waves over
@@ -676,7 +680,7 @@ def batch_comparison(torch, native, dev, steps, warmup, seed=0, meshes=None):
     from slimtracincpp_b200.radiance_cache import RadianceCache
     from slimtracincpp_b200.scene import Scene, geometry
     meshes = meshes if meshes is not None else scenes.config2_meshes()
-    reqs = scenes.config5(seed, meshes=meshes)
+    reqs = scenes.config5(seed, count=count, meshes=meshes, resolutions=resolutions)
     assets = Scene(np.array([geometry(L.GEOMETRY_SPHERE, 0)]), np.array([L.default_material()]), meshes=meshes)
     batch = BatchRenderer(assets)
     RadianceCache.configure(cache_depth=2, train_samples=65536, batch=16384, seed=seed)
@@ -744,7 +748,8 @@ def batch_comparison(torch, native, dev, steps, warmup, seed=0, meshes=None):
         batch.render(sp)
         single_ms.append(sum(timed(3)) / 3)
     ms = sum(batch_ms) / steps
-    return {"workload": "config5_batch_64_requests", "requests": len(reqs), "pixels": pixels,
+    return {"workload": f"config5_batch_{len(reqs)}_requests" + ("_small" if resolutions else ""),
+            "requests": len(reqs), "pixels": pixels,
             "rays_per_batch": rays, "cache_requests": sum(q.radiance_cache != 0 for q in reqs),
             "resolutions": [f"{q.width}x{q.height}" for q in reqs],
             "max_depths": [int(q.settings["max_depth"]) for q in reqs],
@@ -765,7 +770,8 @@ def run_batch_bench(args, torch, dist, dev, rank, world, local):
     clocks.start()
     if world > 1:
         dist.barrier()
-    b = batch_comparison(torch, native, dev, args.steps, args.warmup, args.seed)
+    b = batch_comparison(torch, native, dev, args.steps, args.warmup, args.seed, count=args.batch_requests,
+                         resolutions=[(320, 180), (640, 360)] if args.batch_small else None)
     if world > 1:
         dist.barrier()
     clock_info = clocks.stop()

@@ -506,7 +506,8 @@ def torch_floor8(pix):
     return torch.floor(255.0 * torch.sqrt(pix[:, :3].clamp(0, 1)))
 
 
-def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffixes, seed=0, row_bands=0):
+def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffixes, seed=0, row_bands=0,
+                     overlap=True):
     """Config 4 (config 2's scene at bounce depth 8): plain wavefront
     frames against radiance-cache frames (paths stop at vertex 2; each frame
     trains on `train_samples` paths with four Adam steps of 16,384, then the
@@ -553,7 +554,7 @@ def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffix
     cache_warmup = max(warmup, CACHE_WARMUP_FRAMES)
     for suffix in suffixes:
         cache = RadianceCache.configure(cache_depth=2, train_samples=train_samples, batch=16384, seed=seed,
-                                        train_suffix=suffix)
+                                        train_suffix=suffix, overlap=overlap)
         native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON, row_bands=row_bands)
         outs = buffers(steps)
         for _ in range(cache_warmup):

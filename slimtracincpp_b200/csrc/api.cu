@@ -632,6 +632,10 @@ int check_settings(const Context &c, const SlimRayTracerSettings *st) {
 
 int ensure_wavefront(Context &c, uint32_t samples, int set);
 
+#ifndef SLIM_TRAINING_STREAM_PRIORITY
+#define SLIM_TRAINING_STREAM_PRIORITY 1
+#endif
+
 // Buffers and per-frame parameters of a radiance-cache frame.
 int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     Context::Cache &k = c.cache;
@@ -686,11 +690,15 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     // must be complete when the frame's stream is).
     if (cf.trainer && k.config.overlap && !c.options.count_work && cap) {
         if (!k.stream_b) {
-            // highest priority: the training rounds are long chains of small
-            // launches that should take SMs as soon as the frame's blocks free them
+            // The training stream's priority (SLIM_TRAINING_STREAM_PRIORITY: 1
+            // highest, 0 default, -1 lowest).  Highest: the training rounds are
+            // long chains of small launches that take SMs as soon as the
+            // frame's blocks free them.
             int least = 0, greatest = 0;
             cudaDeviceGetStreamPriorityRange(&least, &greatest);
-            SLIM_CUDA(cudaStreamCreateWithPriority(&k.stream_b, cudaStreamNonBlocking, greatest), "cache training stream");
+            const int priority = SLIM_TRAINING_STREAM_PRIORITY > 0 ? greatest
+                                 : SLIM_TRAINING_STREAM_PRIORITY < 0 ? least : 0;
+            SLIM_CUDA(cudaStreamCreateWithPriority(&k.stream_b, cudaStreamNonBlocking, priority), "cache training stream");
             SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_selected, cudaEventDisableTiming), "cache event");
             SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_trained, cudaEventDisableTiming), "cache event");
         }

@@ -205,7 +205,7 @@ struct Context {
         DevArray<float4> features, aux, radiance, t_features, t_targets, t_color, t_through;
         DevArray<float4> s_features, s_aux, s_radiance;   // self-training queries
         DevArray<uint32_t> s_count;
-        DevArray<float4> q_color, q_through;              // per-query path state
+        DevArray<float4> q_color, q_through, q_hit;       // per-query path state and hit record
         DevArray<uint32_t> counts;
         DevArray<uint32_t> state;      // [0] Adam steps taken, [1] cache frames (training-set offsets)
         uint32_t *error_flags = nullptr;
@@ -649,6 +649,7 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     if ((rc = k.counts.reserve(2, "alloc cache counters"))) return rc;
     if ((rc = k.q_color.reserve(samples, "alloc cache query paths"))) return rc;
     if ((rc = k.q_through.reserve(samples, "alloc cache query paths"))) return rc;
+    if ((rc = k.q_hit.reserve(3 * (size_t)samples, "alloc cache query hits"))) return rc;
     if (cap) {
         if ((rc = k.t_targets.reserve(cap, "alloc training targets"))) return rc;
         if ((rc = k.t_color.reserve(cap, "alloc training paths"))) return rc;
@@ -669,6 +670,7 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     cf.counts = k.counts.ptr;
     cf.q_color = k.q_color.ptr;
     cf.q_through = k.q_through.ptr;
+    cf.q_hit = k.q_hit.ptr;
     cf.train_capacity = cap;
     cf.t_features = k.t_features.ptr;
     cf.t_targets = k.t_targets.ptr;

@@ -98,6 +98,10 @@ struct CacheFrame {
     // throughput), so queries gathered by several row bands -- each with its
     // own path slots -- resolve together (null: read the path slots).
     float4 *q_color = nullptr, *q_through = nullptr;
+    // Each query's hit record (3 float4), copied with the training selection
+    // into the training queues, so training paths start at their cache vertex
+    // without tracing the segment to it again (null: they retrace it).
+    float4 *q_hit = nullptr;
     // Which part of a cache frame a launch runs: the whole frame, the rounds
     // up to the cache vertex and the gather only (a row band), or the cache
     // phase only (once the bands have joined).

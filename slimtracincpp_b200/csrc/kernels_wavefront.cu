@@ -90,6 +90,7 @@ struct CacheArgs {
     uint32_t *frame_counter;
     int mode;
     float4 *q_color, *q_through;   // per query: path colour + depth, throughput (null: path slots)
+    float4 *q_hit;                 // per query: its hit record, 3 float4 (null: not kept)
 };
 
 struct QueueArgs {
@@ -1133,7 +1134,11 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
 }
 
 SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], float3 o, float3 d, uint32_t path,
-                         uint32_t pid, float4 q_color, float4 q_through) {
+                         uint32_t pid, float4 q_color, float4 q_through, const float4 *hit = nullptr) {
+    if (C.q_hit && hit) {
+        float4 *h = C.q_hit + 3 * (size_t)q;
+        h[0] = hit[0]; h[1] = hit[1]; h[2] = hit[2];
+    }
     float4 *p = C.features + 4 * (size_t)q;
     p[0] = f[0]; p[1] = f[1]; p[2] = f[2]; p[3] = f[3];
     C.aux[2 * (size_t)q] = make_float4(o.x, o.y, o.z, __uint_as_float(path));
@@ -1264,7 +1269,7 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
             query = cache_vertex<COUNT, false>(S, F, A, slot, path, pid, o, d, feat, w, qc, qt);
         }
         uint32_t q = warp_append(C.count, query);
-        if (query) append_query(C, q, feat, o, d, path, pid, qc, qt);
+        if (query) append_query(C, q, feat, o, d, path, pid, qc, qt, A.hits + 3 * (size_t)slot);
     }
     flush_stage<COUNT>(A.counters, w);
 }
@@ -1274,7 +1279,7 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
 // more queries than training paths the set is stratified: j takes query
 // floor((j + u) * queries / capacity), u = frac(0.618034 * frame) (a
 // golden-ratio sequence, so consecutive frames train on different queries).
-__global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
+__global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count, float4 *hits) {
     const uint32_t nq = *C.count, cap = C.train_capacity;
     const uint32_t n = nq < cap ? nq : cap;
     const double f = (double)*C.frame_counter * 0.6180339887498949;
@@ -1289,6 +1294,11 @@ __global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count) {
             const float4 *f = C.features + 4 * (size_t)idx;
             float4 *t = C.t_features + 4 * (size_t)j;
             t[0] = f[0]; t[1] = f[1]; t[2] = f[2]; t[3] = f[3];
+        }
+        if (C.q_hit && hits) {   // the query's hit: the training path's first round needs no extend
+            const float4 *h = C.q_hit + 3 * (size_t)idx;
+            float4 *t = hits + 3 * (size_t)j;
+            t[0] = h[0]; t[1] = h[1]; t[2] = h[2];
         }
         float4 a = C.aux[2 * (size_t)idx], b = C.aux[2 * (size_t)idx + 1];
         rays[2 * (size_t)j] = make_float4(a.x, a.y, a.z, __uint_as_float(j));
@@ -1422,7 +1432,7 @@ cudaError_t tail_round(const RoundLaunch &L, QueueArgs &A, uint32_t in, uint32_t
 
 template <bool COUNT, bool BATCH>
 cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA, uint32_t &in, uint32_t depth,
-                        bool primary, bool gather) {
+                        bool primary, bool gather, bool hits_given = false) {
     const WavefrontBuffers &B = *L.B;
     const DevScene &S = *L.S;
     const DevFrame &F = *L.F;
@@ -1439,7 +1449,10 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
     if (r != cudaSuccess) return r;
     A.counters = L.stage(STAGE_EXTEND);
     if (timer) timer->begin(STAGE_EXTEND, stream);
-    if (L.split_extend && B.pair_capacity >= 4) {
+    if (hits_given) {
+        // the queued rays' hit records are in place already (training paths
+        // that start at their cache vertex)
+    } else if (L.split_extend && B.pair_capacity >= 4) {
         // [3] candidates, [4] candidate cursor, [5] overflowed rays
         r = cudaMemsetAsync(B.queue_count + 3, 0, 3 * sizeof(uint32_t), stream);
         if (r != cudaSuccess) return r;
@@ -1553,6 +1566,7 @@ CacheArgs cache_args(const CacheFrame *cache) {
     CA.mode = cache->mode;
     CA.q_color = cache->q_color;
     CA.q_through = cache->q_through;
+    CA.q_hit = cache->q_hit;
     return CA;
 }
 
@@ -1568,20 +1582,26 @@ cudaError_t trace_training(const RoundLaunch &L, QueueArgs &A, const CacheArgs &
     const uint32_t K = cache->depth;
     const bool short_paths = !BATCH && weights && cache->train_suffix && cache->s_count &&
                              K + cache->train_suffix <= max_depth;
+    // the selection copied every training path's hit at the cache vertex
+    const bool hits_given = !BATCH && cache->q_hit;
     if (!short_paths) {
-        if (!L.split_extend) return tail_round<COUNT, BATCH>(L, A, in, K);
-        for (uint32_t depth = K; depth <= max_depth; depth++)
-            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+        if (!L.split_extend && !hits_given) return tail_round<COUNT, BATCH>(L, A, in, K);
+        for (uint32_t depth = K; depth <= max_depth; depth++) {
+            if (!L.split_extend && depth >= kTailDepth && depth > K) return tail_round<COUNT, BATCH>(L, A, in, depth);
+            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) != cudaSuccess)
+                return e;
+        }
         return cudaSuccess;
     }
     const uint32_t last = K + cache->train_suffix;
     for (uint32_t depth = K; depth < last; depth++)
-        if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false)) != cudaSuccess) return e;
+        if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) != cudaSuccess)
+            return e;
     CacheArgs SC = CA;
     SC.features = cache->s_features;
     SC.aux = cache->s_aux;
     SC.count = cache->s_count;
-    SC.q_color = SC.q_through = nullptr;
+    SC.q_color = SC.q_through = SC.q_hit = nullptr;   // the frame's own query records stay untouched
     if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
     if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
     if ((e = nrc::launch_infer(cache->s_features, cache->s_count, 0, cache->train_capacity, cache->s_radiance, weights,
@@ -1623,7 +1643,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (timer) timer->begin(STAGE_CACHE, stream);
         uint32_t g = (cache->train_capacity + 255) / 256;
         if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
-        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, TB.rays[0], TB.queue_count);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, TB.rays[0], TB.queue_count, TB.hits);
         count_launch();
         if (timer) timer->end(STAGE_CACHE, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1656,7 +1676,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (timer) timer->begin(STAGE_CACHE, stream);
         uint32_t g = (cache->train_capacity + 255) / 256;
         if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
-        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in, B.hits);
         count_launch();
         if (timer) timer->end(STAGE_CACHE, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -517,9 +517,18 @@ int sm_count() {
 }
 }  // namespace
 
+// CTAs of a training step: one per 128-sample tile up to one per SM, or at
+// most SLIM_NRC_TRAIN_MAX_CTAS when that is set (each CTA then loops over
+// several tiles).  A training CTA holds 166 KB of shared memory, which on its
+// SM is taken from the L1 cache the traversal kernels running beside an
+// overlapped training step read their nodes through.
+#ifndef SLIM_NRC_TRAIN_MAX_CTAS
+#define SLIM_NRC_TRAIN_MAX_CTAS 0
+#endif
 int train_grid(uint32_t samples) {
     uint32_t tiles = (samples + kTile - 1) / kTile;
     uint32_t g = (uint32_t)sm_count();
+    if (SLIM_NRC_TRAIN_MAX_CTAS > 0 && g > (uint32_t)SLIM_NRC_TRAIN_MAX_CTAS) g = SLIM_NRC_TRAIN_MAX_CTAS;
     return (int)(tiles < g ? (tiles ? tiles : 1) : g);
 }
 

@@ -194,8 +194,14 @@ __global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
 // ended writes its pixel, and the idle lanes of the warp claim the next
 // pixels of the queue together (one atomic per warp, ranks by ballot), so
 // warps stay full until the queue is empty whatever the path lengths.
+// Blocks per SM the persistent batch kernel is compiled for (a register cap:
+// its walks wait on dependent loads, so warps can beat registers).
+#ifndef SLIM_BATCH_PERSISTENT_MIN_BLOCKS
+#define SLIM_BATCH_PERSISTENT_MIN_BLOCKS 1
+#endif
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_batch_persistent(const DevScene *scenes, const DevFrame *frames,
+__global__ void __launch_bounds__(128, SLIM_BATCH_PERSISTENT_MIN_BLOCKS)
+k_batch_persistent(const DevScene *scenes, const DevFrame *frames,
                                                           const uint32_t *requests, const uint32_t *prefix,
                                                           uint32_t count, uint32_t total, uint32_t *cursor,
                                                           uint32_t *error_flags, unsigned long long *counters) {

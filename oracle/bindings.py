@@ -131,7 +131,62 @@ def reference_host_builders(layout, lib=None):
     def projection(camera, width, height, ssaa):
         return reference_projection(camera, width, height, ssaa, layout, lib=h)
 
-    return {"scene_bvh": scene_bvh, "mesh": mesh, "projection": projection}
+    out = {"scene_bvh": scene_bvh, "mesh": mesh, "projection": projection}
+    if BMP2TEXTURE.exists():
+        out["texture"] = lambda bgr, flags: reference_bake_texture(bgr, flags, layout)
+    return out
+
+
+BMP2TEXTURE = HERE / "_ref" / "bmp2texture"
+
+
+def write_bmp(path, bgr, top_down=True):
+    """A BMP of 8-bit B,G,R(,A) rows as the reference's loader reads them
+    (rows read back to back: 24-bit rows must be 4-byte multiples)."""
+    import struct
+    h, w, ch = bgr.shape
+    rows = bgr if top_down else bgr[::-1]
+    data = np.ascontiguousarray(rows).tobytes()
+    off = 14 + 40
+    head = struct.pack("<2sIHHI", b"BM", off + len(data), 0, 0, off)
+    info = struct.pack("<IiiHHIIiiII", 40, w, -h if top_down else h, 1, 8 * ch, 0, len(data), 2835, 2835, 0, 0)
+    Path(path).write_bytes(head + info + data)
+
+
+def read_texture_file(path, layout):
+    """A .texture file (ImageInfo, then per mip u32 width, height and its
+    texel quads) as (Texture record, mip sizes, texel quads)."""
+    b = Path(path).read_bytes()
+    buf = np.zeros(1, layout.TEXTURE)
+    buf.view(np.uint8)[:32] = np.frombuffer(b[:32], np.uint8)
+    header = buf[0]
+    off, sizes, chunks = 32, [], []
+    for _ in range(int(header["mip_count"])):
+        w, h = np.frombuffer(b[off:off + 8], np.uint32)
+        off += 8
+        n = (int(w) + 1) * (int(h) + 1) * layout.TEXEL_QUAD.itemsize
+        chunks.append(np.frombuffer(b[off:off + n], layout.TEXEL_QUAD))
+        off += n
+        sizes.append((int(w), int(h)))
+    return header, sizes, np.concatenate(chunks)
+
+
+def reference_bake_texture(bgr, flags, layout):
+    """The reference's own converter (oracle/_ref/bmp2texture) on 8-bit
+    BGR(A) rows: the image goes through a BMP file and the switches the
+    flags name (-l -m -w -n -c)."""
+    import subprocess
+    import tempfile
+    img = np.ascontiguousarray(bgr, dtype=np.uint8)
+    if (img.shape[1] * img.shape[2]) % 4:
+        raise ValueError("the reference's BMP loader needs rows of a multiple of 4 bytes")
+    switches = [s for bit, s in ((layout.IMAGE_LINEAR, "-l"), (layout.IMAGE_MIPMAP, "-m"), (layout.IMAGE_WRAP, "-w"),
+                                 (layout.IMAGE_NORMAL, "-n"), (layout.IMAGE_CUBEMAP, "-c")) if flags & bit]
+    with tempfile.TemporaryDirectory() as d:
+        bmp, tex = Path(d) / "t.bmp", Path(d) / "t.texture"
+        write_bmp(bmp, img)
+        subprocess.run([str(BMP2TEXTURE), str(bmp), str(tex), *switches], check=True, timeout=600)
+        return read_texture_file(tex, layout)
 
 
 def make_canvas(width, height, antialias, layout):

@@ -18,6 +18,7 @@ from .native import check, lib, ptr
 #   "mesh"        f(positions, indices, normals, normal_indices, uvs, uv_indices)
 #                   -> (triangles, nodes, height, aabb6, recentred positions)
 #   "projection"  f(camera, width, height, ssaa) -> CameraRayProjection record
+#   "texture"     f(bgr rows, flags) -> (Texture record, mip sizes, texel quads)
 HOST_BUILDERS = {}
 
 
@@ -162,6 +163,9 @@ class TextureAsset:
         """bmp2texture's baker (bmp2texture.cpp:24-335) on 8-bit BGR(A) rows,
         on the host or (on_gpu) on the device: the same bytes."""
         img = np.ascontiguousarray(bgr, dtype=np.uint8)
+        if "texture" in HOST_BUILDERS and not on_gpu:
+            header, sizes, quads = HOST_BUILDERS["texture"](img, flags)
+            return cls(header, sizes, quads)
         h, w, ch = img.shape
         mip_count = np.zeros(1, np.uint32)
         quad_count = np.zeros(1, np.uint32)

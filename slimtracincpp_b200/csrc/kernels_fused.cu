@@ -195,9 +195,11 @@ __global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
 // pixels of the queue together (one atomic per warp, ranks by ballot), so
 // warps stay full until the queue is empty whatever the path lengths.
 // Blocks per SM the persistent batch kernel is compiled for (a register cap:
-// its walks wait on dependent loads, so warps can beat registers).
+// its walks wait on dependent loads, so warps beat registers; config 5's
+// plain requests in one launch: 84.3 ms uncapped at 168 registers, 74.7 ms
+// at 6 blocks, 77.0 ms at 8).
 #ifndef SLIM_BATCH_PERSISTENT_MIN_BLOCKS
-#define SLIM_BATCH_PERSISTENT_MIN_BLOCKS 1
+#define SLIM_BATCH_PERSISTENT_MIN_BLOCKS 6
 #endif
 template <bool COUNT>
 __global__ void __launch_bounds__(128, SLIM_BATCH_PERSISTENT_MIN_BLOCKS)

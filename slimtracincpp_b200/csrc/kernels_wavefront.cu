@@ -1635,9 +1635,10 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         // answers the queries and the next frame's primary rays run.
         const WavefrontBuffers &TB = *cache->train_queues;
         cudaStream_t ts = cache->train_stream;
-        if ((e = cudaStreamWaitEvent(stream, cache->trained, 0)) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync((void *)cache->weights, cache->train_weights, nrc::kImgBytes, cudaMemcpyDeviceToDevice,
-                                 stream)) != cudaSuccess)
+        const bool lag2 = cache->weights_ready && cache->weights_source && cache->publish && cache->published;
+        if ((e = cudaStreamWaitEvent(stream, lag2 ? cache->weights_ready : cache->trained, 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync((void *)cache->weights, lag2 ? cache->weights_source : cache->train_weights,
+                                 nrc::kImgBytes, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
             return e;
         if ((e = cudaMemsetAsync(TB.queue_count, 0, 8 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
         if (timer) timer->begin(STAGE_CACHE, stream);
@@ -1670,6 +1671,12 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
             if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, ts)) !=
                 cudaSuccess)
                 return e;
+        }
+        if (lag2) {
+            if ((e = cudaMemcpyAsync(cache->publish, cache->train_weights, nrc::kImgBytes, cudaMemcpyDeviceToDevice,
+                                     ts)) != cudaSuccess)
+                return e;
+            if ((e = cudaEventRecord(cache->published, ts)) != cudaSuccess) return e;
         }
         if ((e = cudaEventRecord(cache->trained, ts)) != cudaSuccess) return e;
     } else if (mode == SLIM_CACHE_EXACT || train) {

@@ -980,7 +980,7 @@ def main():
         # the metric's second half, in the same process: config 4 (this scene at
         # bounce depth 8), plain frames against radiance-cache frames
         w4 = scenes.config4(args.seed, meshes=w.scene.meshes)
-        cmp = cache_comparison(torch, native, w4, dev, min(args.steps, 10), args.warmup, args.train_samples, [0, 1],
+        cmp = cache_comparison(torch, native, w4, dev, args.steps, args.warmup, args.train_samples, [0, 1],
                                args.seed)
         cmp["workload"] = w4.name
         cmp["nrc_roofline"] = nrc_roofline(torch, native, w4, dev)

@@ -254,7 +254,7 @@ TRAFFIC_BYTES_PER_LAUNCH = {
     ("config2", "shadow_mesh"): 61.6e6,   # 93.0 MB and 30.2 MB
 }
 PIXEL_STAGES = ("shade", "tail", "fused")   # stages that write the framebuffer
-CACHE_WARMUP_FRAMES = 16   # radiance-cache frames trained before the timed ones
+CACHE_WARMUP_FRAMES = 32   # radiance-cache frames trained before the timed ones
 
 
 def measured_peaks():
@@ -550,6 +550,15 @@ def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffix
     plain_ms = timed_frames(torch, native, r, vp, sp, stream, ref * steps, flush)
     out = {"plain_depth8": {"ms_per_frame": sum(plain_ms) / steps, "rays_per_frame": plain_rays,
                             "mrays_s": plain_rays / (sum(plain_ms) / steps / 1000.0) / 1e6}, "cache": []}
+    # the ablation: the same frame with the paths cut at the cache vertex and nothing added
+    RadianceCache.configure(cache_depth=2, train_samples=train_samples, batch=16384, seed=seed, train=False)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_TRUNCATE)
+    trunc = buffers(1)
+    native.check(lib.slimRefitSceneBVH(sp))
+    r.render_to_device(vp, trunc[0][0].data_ptr(), trunc[0][1].data_ptr(), sp)
+    torch.cuda.synchronize()
+    tq = frame_quality(trunc[0][0], ref[0][0])
+    out["truncated_at_cache_vertex"] = {"psnr_db": tq[0], "max_abs": tq[1]}
     cache_warmup = max(warmup, CACHE_WARMUP_FRAMES)
     for suffix in suffixes:
         cache = RadianceCache.configure(cache_depth=2, train_samples=train_samples, batch=16384, seed=seed,

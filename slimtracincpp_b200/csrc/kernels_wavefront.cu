@@ -35,6 +35,16 @@ namespace dev {
 
 SLIM_D uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Persistent mesh walks (SLIM_MESH_PREFETCH = 1): the child pair a step
+// pushes for later and the triangles of a leaf it parks are prefetched into
+// L1, so the pop and the leaf test that come turns later find them there.
+#ifndef SLIM_MESH_PREFETCH
+#define SLIM_MESH_PREFETCH 0
+#endif
+SLIM_D void prefetch_l1(const void *p) {
+    if (SLIM_MESH_PREFETCH) asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 // Warp-aggregated queue append: one atomicAdd per warp, slots handed out
 // by the ballot's prefix popcount.  Returns the slot of a thread whose
 // `want` is set.
@@ -613,11 +623,12 @@ __global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFr
             bool hr = hit_node(r, xa, xb, rn, rf) && rn < aux;
             uint32_t lc = node_first(lb), rc = node_first(xb);
             uint32_t lcount = node_leaf_count(lb), rcount = node_leaf_count(xb);
-            if (hl && lcount) pend.push(lc, lcount, lf);
-            if (hr && rcount) pend.push(rc, rcount, rf);
+            if (hl && lcount) { pend.push(lc, lcount, lf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + lc)); }
+            if (hr && rcount) { pend.push(rc, rcount, rf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + rc)); }
             bool go_left = hl && !lcount, go_right = hr && !rcount;
             if (go_left) {
                 if (go_right) {
+                    prefetch_l1(nodes + 2 * (size_t)rc);
                     if (!push_entry(stack, bottom, top, rc)) { err |= kErrStack; walking = false; }
                 }
                 left = lc;
@@ -894,12 +905,13 @@ __global__ void __launch_bounds__(kMeshBlock, 7) k_extend_mesh(DevScene S, DevFr
             bool hr = hit_node(r, xa, xb, rn, rf) && rn < lc && rn <= gb;
             uint32_t lchild = node_first(lb), rchild = node_first(xb);
             uint32_t lcount = node_leaf_count(lb), rcount = node_leaf_count(xb);
-            if (hl && lcount) pend.push(lchild, lcount, lf);
-            if (hr && rcount) pend.push(rchild, rcount, rf);
+            if (hl && lcount) { pend.push(lchild, lcount, lf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + lchild)); }
+            if (hr && rcount) { pend.push(rchild, rcount, rf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + rchild)); }
             bool go_left = hl && !lcount, go_right = hr && !rcount;
             if (go_left) {
                 if (go_right) {
                     if (ln > rn) { uint32_t t = lchild; lchild = rchild; rchild = t; }
+                    prefetch_l1(nodes + 2 * (size_t)rchild);
                     if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; walking = false; }
                     else stack[top++] = rchild;
                 }

@@ -41,6 +41,11 @@ SLIM_D uint32_t lane_id() { return threadIdx.x & 31u; }
 #ifndef SLIM_MESH_PREFETCH
 #define SLIM_MESH_PREFETCH 0
 #endif
+// Overlapped cache training: its trace rounds launch for at most this many
+// SMs' worth of blocks (0: all), leaving the rest to the next frame's rays.
+#ifndef SLIM_CACHE_TRAIN_SMS
+#define SLIM_CACHE_TRAIN_SMS 0
+#endif
 SLIM_D void prefetch_l1(const void *p) {
     if (SLIM_MESH_PREFETCH) asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
@@ -1394,6 +1399,7 @@ struct RoundLaunch {
     uint32_t lights;     // most lights of any scene in the round
     bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
+    uint32_t sm_cap = 0;     // launch for at most this many SMs' worth of blocks (0: all SMs)
     cudaEvent_t pixel_wait = nullptr;  // kernels that write pixels wait for it (a download in flight)
     const FrameDownload *depth_download = nullptr;  // first round: the depths download after shadow_gen
     const FrameDownload *pixel_download = nullptr;  // first round: each shade chunk's rows download after it
@@ -1405,7 +1411,8 @@ struct RoundLaunch {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
         if (share_sms && per_sm > 1) per_sm--;
-        uint32_t g = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
+        const uint32_t s = sm_cap && sm_cap < (uint32_t)sms ? sm_cap : (uint32_t)sms;
+        uint32_t g = s * (uint32_t)(per_sm > 0 ? per_sm : 1);
         uint32_t need = (work + block - 1) / block;
         return need < g ? (need ? need : 1) : g;
     }
@@ -1663,6 +1670,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if ((e = cudaEventRecord(cache->selected, stream)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(ts, cache->selected, 0)) != cudaSuccess) return e;
         RoundLaunch TL{L.S, L.F, &TB, L.block, L.sms, ts, nullptr, nullptr, TB.capacity, L.lights, L.split_extend};
+        TL.sm_cap = SLIM_CACHE_TRAIN_SMS;
         QueueArgs TA = A;
         TA.hits = TB.hits;
         TA.shadow_rays = TB.shadow_rays;

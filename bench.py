@@ -507,6 +507,8 @@ def torch_floor8(pix):
 
 def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffixes, seed=0, row_bands=0,
                      overlap=True):
+    """`suffixes`: training suffixes (with `train_samples` paths per frame),
+    or (suffix, train samples) pairs."""
     """Config 4 (config 2's scene at bounce depth 8): plain wavefront
     frames against radiance-cache frames (paths stop at vertex 2; each frame
     trains on `train_samples` paths with four Adam steps of 16,384, then the
@@ -560,8 +562,9 @@ def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffix
     tq = frame_quality(trunc[0][0], ref[0][0])
     out["truncated_at_cache_vertex"] = {"psnr_db": tq[0], "max_abs": tq[1]}
     cache_warmup = max(warmup, CACHE_WARMUP_FRAMES)
-    for suffix in suffixes:
-        cache = RadianceCache.configure(cache_depth=2, train_samples=train_samples, batch=16384, seed=seed,
+    for variant in suffixes:
+        suffix, samples = variant if isinstance(variant, tuple) else (variant, train_samples)
+        cache = RadianceCache.configure(cache_depth=2, train_samples=samples, batch=16384, seed=seed,
                                         train_suffix=suffix, overlap=overlap)
         native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON, row_bands=row_bands)
         outs = buffers(steps)
@@ -585,7 +588,8 @@ def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffix
         out["cache"].append({
             "train_targets": "full-depth paths traced by the tracer (as specified)" if suffix == 0 else
                              f"self-training: {suffix} bounce(s) past the cache vertex, then the cache's own answer",
-            "train_suffix": suffix, "ms_per_frame": total / steps, "rays_per_frame": rays,
+            "train_suffix": suffix, "train_samples_per_frame": samples, "ms_per_frame": total / steps,
+            "rays_per_frame": rays,
             "speedup_vs_plain_depth8": (sum(plain_ms) / steps) / (total / steps),
             "psnr_db_per_frame": [q[0] for q in quality], "max_abs_per_frame": [q[1] for q in quality],
             "min_psnr_db": min(q[0] for q in quality), "frame_event_ms": frame_ms,
@@ -989,7 +993,8 @@ def main():
         # the metric's second half, in the same process: config 4 (this scene at
         # bounce depth 8), plain frames against radiance-cache frames
         w4 = scenes.config4(args.seed, meshes=w.scene.meshes)
-        cmp = cache_comparison(torch, native, w4, dev, args.steps, args.warmup, args.train_samples, [0, 1],
+        cmp = cache_comparison(torch, native, w4, dev, args.steps, args.warmup, args.train_samples,
+                               [0, 1, (1, args.train_samples // 2)],
                                args.seed)
         cmp["workload"] = w4.name
         cmp["nrc_roofline"] = nrc_roofline(torch, native, w4, dev)

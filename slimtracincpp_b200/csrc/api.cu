@@ -213,10 +213,6 @@ struct Context {
         cudaStream_t stream_b = nullptr;
         cudaEvent_t ev_selected = nullptr, ev_trained = nullptr;
         DevArray<uint8_t> image_infer;
-        // two frames of weight lag: images published by alternate frames' training
-        DevArray<uint8_t> published[2];
-        cudaEvent_t ev_published[2] = {nullptr, nullptr};
-        uint32_t publish_parity = 0;
         DevArray<float4> tq_rays0, tq_rays1, tq_hits, tq_shadow, tq_pairs;
         DevArray<uint32_t> tq_counts;
         DevArray<unsigned long long> tq_masks;
@@ -636,19 +632,9 @@ int check_settings(const Context &c, const SlimRayTracerSettings *st) {
 
 int ensure_wavefront(Context &c, uint32_t samples, int set);
 
-#ifndef SLIM_TRAINING_STREAM_PRIORITY
-#define SLIM_TRAINING_STREAM_PRIORITY 1
-#endif
-// Frames between the training whose weights a cache frame's queries use and
-// the frame: 1 (the previous frame's training; the frame waits for it to end
-// before it answers its queries) or 2 (the training before that, which has
-// had a whole frame more to finish).
-#ifndef SLIM_CACHE_WEIGHT_LAG
-#define SLIM_CACHE_WEIGHT_LAG 1
-#endif
 
 // Buffers and per-frame parameters of a radiance-cache frame.
-int cache_frame(Context &c, uint32_t samples, CacheFrame &cf, int part) {
+int cache_frame(Context &c, uint32_t samples, CacheFrame &cf) {
     Context::Cache &k = c.cache;
     if (!k.configured) return set_error(SLIM_ERR_STATE, "radiance_cache is set but slimRadianceCacheConfigure was not called");
     const int mode = c.options.radiance_cache;
@@ -703,15 +689,12 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf, int part) {
     // must be complete when the frame's stream is).
     if (cf.trainer && k.config.overlap && !c.options.count_work && cap) {
         if (!k.stream_b) {
-            // The training stream's priority (SLIM_TRAINING_STREAM_PRIORITY: 1
-            // highest, 0 default, -1 lowest).  Highest: the training rounds are
-            // long chains of small launches that take SMs as soon as the
-            // frame's blocks free them.
+            // highest priority: the training rounds are long chains of small
+            // launches that should take SMs as soon as the frame's blocks free
+            // them (default and lowest priority measured the same)
             int least = 0, greatest = 0;
             cudaDeviceGetStreamPriorityRange(&least, &greatest);
-            const int priority = SLIM_TRAINING_STREAM_PRIORITY > 0 ? greatest
-                                 : SLIM_TRAINING_STREAM_PRIORITY < 0 ? least : 0;
-            SLIM_CUDA(cudaStreamCreateWithPriority(&k.stream_b, cudaStreamNonBlocking, priority), "cache training stream");
+            SLIM_CUDA(cudaStreamCreateWithPriority(&k.stream_b, cudaStreamNonBlocking, greatest), "cache training stream");
             SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_selected, cudaEventDisableTiming), "cache event");
             SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_trained, cudaEventDisableTiming), "cache event");
         }
@@ -746,22 +729,6 @@ int cache_frame(Context &c, uint32_t samples, CacheFrame &cf, int part) {
         cf.train_queues = &k.tq;
         cf.train_weights = k.image.ptr;
         cf.weights = k.image_infer.ptr;
-        if (SLIM_CACHE_WEIGHT_LAG == 2) {
-            for (int i = 0; i < 2; i++) {
-                if (!k.published[i].ptr) {
-                    if ((rc = k.published[i].reserve(nrc::kImgBytes, "alloc published weights"))) return rc;
-                    SLIM_CUDA(cudaMemcpy(k.published[i].ptr, k.image.ptr, nrc::kImgBytes, cudaMemcpyDeviceToDevice),
-                              "init published weights");
-                    SLIM_CUDA(cudaEventCreateWithFlags(&k.ev_published[i], cudaEventDisableTiming), "cache event");
-                }
-            }
-            const uint32_t p = k.publish_parity;
-            cf.publish = k.published[p].ptr;
-            cf.published = k.ev_published[p];
-            cf.weights_source = k.published[p ^ 1u].ptr;
-            cf.weights_ready = k.ev_published[p ^ 1u];
-            if (part != kCachePartGather) k.publish_parity ^= 1u;   // once per frame: the call that trains
-        }
     }
     return SLIM_OK;
 }
@@ -829,7 +796,7 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
         CacheFrame cf;
         const CacheFrame *cache = nullptr;
         if (c.options.radiance_cache != SLIM_CACHE_OFF) {
-            if ((rc = cache_frame(c, F.width * F.height, cf, cache_part))) return rc;
+            if ((rc = cache_frame(c, F.width * F.height, cf))) return rc;
             cf.part = cache_part;
             cache = &cf;
         }
@@ -1046,7 +1013,7 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     if (cache_bands) {
         // the frame's query buffers, and its query count cleared once for all bands
         CacheFrame cf;
-        if ((rc = cache_frame(c, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1), cf, kCachePartGather))) return rc;
+        if ((rc = cache_frame(c, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1), cf))) return rc;
         SLIM_CUDA(cudaMemsetAsync(cf.counts, 0, sizeof(uint32_t), stream), "clear cache queries");
     }
     SLIM_CUDA(cudaEventRecord(c.band_fork, stream), "band fork");
@@ -1624,10 +1591,6 @@ int upload_cache_weights(Context &c, const float *params) {
     SLIM_CUDA(cudaMemset(k.loss.ptr, 0, sizeof(float)), "clear loss");
     SLIM_CUDA(nrc::launch_pack_weights(k.params.ptr, k.image.ptr, nullptr), "pack weights");
     SLIM_CUDA(cudaMemset(k.state.ptr, 0, sizeof(uint32_t)), "clear step count");
-    for (int i = 0; i < 2; i++)   // published images of a two-frame lag start from the new weights too
-        if (k.published[i].ptr)
-            SLIM_CUDA(cudaMemcpy(k.published[i].ptr, k.image.ptr, nrc::kImgBytes, cudaMemcpyDeviceToDevice),
-                      "reset published weights");
     return cache_sync_errors(c);
 }
 

@@ -88,13 +88,6 @@ struct CacheFrame {
     const WavefrontBuffers *train_queues = nullptr;
     const uint8_t *train_weights = nullptr;   // image the training updates; copied into `weights`
                                               // (what the queries read) once per frame
-    // Two frames of lag (null: one): the queries' snapshot is copied from
-    // `weights_source` once `weights_ready` (the training of two frames
-    // ago) has completed, and this frame's training ends by publishing its
-    // image into `publish` and recording `published`.
-    cudaEvent_t weights_ready = nullptr, published = nullptr;
-    const uint8_t *weights_source = nullptr;
-    uint8_t *publish = nullptr;
     // Self-training (train_suffix > 0): the training paths stop train_suffix
     // bounces past the cache vertex and query the cache there; those queries
     // go to their own buffers (one slot per training path).

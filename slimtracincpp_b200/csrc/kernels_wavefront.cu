@@ -35,20 +35,7 @@ namespace dev {
 
 SLIM_D uint32_t lane_id() { return threadIdx.x & 31u; }
 
-// Persistent mesh walks (SLIM_MESH_PREFETCH = 1): the child pair a step
-// pushes for later and the triangles of a leaf it parks are prefetched into
-// L1, so the pop and the leaf test that come turns later find them there.
-#ifndef SLIM_MESH_PREFETCH
-#define SLIM_MESH_PREFETCH 0
-#endif
-// Overlapped cache training: its trace rounds launch for at most this many
-// SMs' worth of blocks (0: all), leaving the rest to the next frame's rays.
-#ifndef SLIM_CACHE_TRAIN_SMS
-#define SLIM_CACHE_TRAIN_SMS 0
-#endif
-SLIM_D void prefetch_l1(const void *p) {
-    if (SLIM_MESH_PREFETCH) asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
+
 
 // Warp-aggregated queue append: one atomicAdd per warp, slots handed out
 // by the ballot's prefix popcount.  Returns the slot of a thread whose
@@ -628,12 +615,11 @@ __global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFr
             bool hr = hit_node(r, xa, xb, rn, rf) && rn < aux;
             uint32_t lc = node_first(lb), rc = node_first(xb);
             uint32_t lcount = node_leaf_count(lb), rcount = node_leaf_count(xb);
-            if (hl && lcount) { pend.push(lc, lcount, lf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + lc)); }
-            if (hr && rcount) { pend.push(rc, rcount, rf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + rc)); }
+            if (hl && lcount) pend.push(lc, lcount, lf);
+            if (hr && rcount) pend.push(rc, rcount, rf);
             bool go_left = hl && !lcount, go_right = hr && !rcount;
             if (go_left) {
                 if (go_right) {
-                    prefetch_l1(nodes + 2 * (size_t)rc);
                     if (!push_entry(stack, bottom, top, rc)) { err |= kErrStack; walking = false; }
                 }
                 left = lc;
@@ -910,13 +896,12 @@ __global__ void __launch_bounds__(kMeshBlock, 7) k_extend_mesh(DevScene S, DevFr
             bool hr = hit_node(r, xa, xb, rn, rf) && rn < lc && rn <= gb;
             uint32_t lchild = node_first(lb), rchild = node_first(xb);
             uint32_t lcount = node_leaf_count(lb), rcount = node_leaf_count(xb);
-            if (hl && lcount) { pend.push(lchild, lcount, lf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + lchild)); }
-            if (hr && rcount) { pend.push(rchild, rcount, rf); prefetch_l1(S.tri_hot + 3 * (size_t)(tri_offset + rchild)); }
+            if (hl && lcount) pend.push(lchild, lcount, lf);
+            if (hr && rcount) pend.push(rchild, rcount, rf);
             bool go_left = hl && !lcount, go_right = hr && !rcount;
             if (go_left) {
                 if (go_right) {
                     if (ln > rn) { uint32_t t = lchild; lchild = rchild; rchild = t; }
-                    prefetch_l1(nodes + 2 * (size_t)rchild);
                     if (top >= (uint32_t)kStackCapacity) { err |= kErrStack; walking = false; }
                     else stack[top++] = rchild;
                 }
@@ -1399,7 +1384,6 @@ struct RoundLaunch {
     uint32_t lights;     // most lights of any scene in the round
     bool split_extend;   // closest hits as scene candidates + the persistent mesh pass
     bool share_sms = false;  // leave a block's room per SM (overlapped cache training runs beside)
-    uint32_t sm_cap = 0;     // launch for at most this many SMs' worth of blocks (0: all SMs)
     cudaEvent_t pixel_wait = nullptr;  // kernels that write pixels wait for it (a download in flight)
     const FrameDownload *depth_download = nullptr;  // first round: the depths download after shadow_gen
     const FrameDownload *pixel_download = nullptr;  // first round: each shade chunk's rows download after it
@@ -1411,8 +1395,7 @@ struct RoundLaunch {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
         if (share_sms && per_sm > 1) per_sm--;
-        const uint32_t s = sm_cap && sm_cap < (uint32_t)sms ? sm_cap : (uint32_t)sms;
-        uint32_t g = s * (uint32_t)(per_sm > 0 ? per_sm : 1);
+        uint32_t g = (uint32_t)(sms * (per_sm > 0 ? per_sm : 1));
         uint32_t need = (work + block - 1) / block;
         return need < g ? (need ? need : 1) : g;
     }
@@ -1654,10 +1637,9 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         // answers the queries and the next frame's primary rays run.
         const WavefrontBuffers &TB = *cache->train_queues;
         cudaStream_t ts = cache->train_stream;
-        const bool lag2 = cache->weights_ready && cache->weights_source && cache->publish && cache->published;
-        if ((e = cudaStreamWaitEvent(stream, lag2 ? cache->weights_ready : cache->trained, 0)) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync((void *)cache->weights, lag2 ? cache->weights_source : cache->train_weights,
-                                 nrc::kImgBytes, cudaMemcpyDeviceToDevice, stream)) != cudaSuccess)
+        if ((e = cudaStreamWaitEvent(stream, cache->trained, 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync((void *)cache->weights, cache->train_weights, nrc::kImgBytes, cudaMemcpyDeviceToDevice,
+                                 stream)) != cudaSuccess)
             return e;
         if ((e = cudaMemsetAsync(TB.queue_count, 0, 8 * sizeof(uint32_t), stream)) != cudaSuccess) return e;
         if (timer) timer->begin(STAGE_CACHE, stream);
@@ -1670,7 +1652,6 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if ((e = cudaEventRecord(cache->selected, stream)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(ts, cache->selected, 0)) != cudaSuccess) return e;
         RoundLaunch TL{L.S, L.F, &TB, L.block, L.sms, ts, nullptr, nullptr, TB.capacity, L.lights, L.split_extend};
-        TL.sm_cap = SLIM_CACHE_TRAIN_SMS;
         QueueArgs TA = A;
         TA.hits = TB.hits;
         TA.shadow_rays = TB.shadow_rays;
@@ -1691,12 +1672,6 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
             if ((e = cache->trainer->step(cache->t_features, cache->t_targets, n, cache->counts + 1, off, ts)) !=
                 cudaSuccess)
                 return e;
-        }
-        if (lag2) {
-            if ((e = cudaMemcpyAsync(cache->publish, cache->train_weights, nrc::kImgBytes, cudaMemcpyDeviceToDevice,
-                                     ts)) != cudaSuccess)
-                return e;
-            if ((e = cudaEventRecord(cache->published, ts)) != cudaSuccess) return e;
         }
         if ((e = cudaEventRecord(cache->trained, ts)) != cudaSuccess) return e;
     } else if (mode == SLIM_CACHE_EXACT || train) {

@@ -23,99 +23,6 @@ SLIM_D void flush_work(unsigned long long *counters, const Work &w) {
     }
 }
 
-// renderPixelBeauty (renderer/ray_tracer.h:19-108) as a sequence of path
-// segments: a path's state between two segments is the ray of the next one,
-// the colour and throughput so far, the canvas depth and the bounces left.
-struct PathState {
-    float3 o, d;
-    float3 color, throughput;
-    float depth, scaling;
-    uint32_t depth_left;
-};
-
-template <bool COUNT>
-SLIM_D void path_start(const DevFrame &F, int x, int y, PathState &p, Work &w) {
-    const SlimCameraRayProjection &P = F.projection;
-    p.scaling = F.cones_per_pixel ? pixel_scaling(P, x, y) : 0.0f;
-    p.o = f3(P.camera_position.x, P.camera_position.y, P.camera_position.z);
-    p.d = normalized(primary_direction(P, x, y));
-    bump<COUNT>(w.primary);
-    p.color = f3(0, 0, 0);
-    p.throughput = f3(1, 1, 1);
-    p.depth = INFINITY;
-    p.depth_left = F.settings.max_depth;
-}
-
-// One segment: closest hit, shading (point lights with their shadow rays,
-// area lights, IBL), the bounce decision, the light glow of the segment.
-// Returns whether the path goes on.
-template <bool COUNT>
-SLIM_D bool path_segment(const DevScene &S, const DevFrame &F, PathState &p, uint32_t *stack, uint32_t *mesh_stack,
-                         uint32_t &err, Work &w) {
-    const SlimRayTracerSettings &st = F.settings;
-    Ray ray;
-    reset(ray, p.o, p.d);
-    Hit hit;
-    Surface s;
-    float3 current = f3(0, 0, 0), next_throughput = f3(0, 0, 0);
-    int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
-    if (g >= 0) {
-        Geo geo = load_geo(S, (uint32_t)g);
-        Mat m = load_mat(S, geo.material);
-        if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
-            p.depth_left = 0;
-            current = m.emission;
-        } else {
-            prepare_for_shading<COUNT>(S, geo, m, ray, hit, p.scaling, s, w);
-            if (p.depth_left == st.max_depth) p.depth = depth_at(F.projection, hit.position);
-            for (uint32_t i = 0; i < S.light_count; i++) {
-                LightRec l = load_light(S, i);
-                if (!is_facing_light(s, l)) continue;
-                if (l.flags & SLIM_LIGHT_IS_SHADOWING) {
-                    Ray sr;
-                    sr.o = s.P;
-                    sr.d = s.L;
-                    Hit sh;
-                    bump<COUNT>(w.shadow);
-                    const uint32_t sn = w.scene_nodes, mn = w.mesh_nodes, tr = w.triangles, ge = w.geometries;
-                    const bool occluded = scene_trace<COUNT>(S, sr, sh, true, s.Ld, stack, mesh_stack, err, w) >= 0;
-                    bump<COUNT>(w.any_scene_nodes, w.scene_nodes - sn);
-                    bump<COUNT>(w.any_mesh_nodes, w.mesh_nodes - mn);
-                    bump<COUNT>(w.any_triangles, w.triangles - tr);
-                    bump<COUNT>(w.any_geometries, w.geometries - ge);
-                    if (occluded) continue;
-                }
-                add_light(s, m, l, current);
-            }
-            if (S.flags & SLIM_SCENE_HAD_EMISSIVE_QUADS) shade_from_emissive_quads(S, g, s, m, current);
-            if (st.skybox_irradiance_texture_id >= 0 && st.skybox_radiance_texture_id >= 0) {
-                s.L = s.N;
-                s.NdotL = 1.0f;
-                float3 D = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_irradiance_texture_id, s.N.x, s.N.y, s.N.z, w);
-                float3 Sp = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_radiance_texture_id, s.R.x, s.R.y, s.R.z, w);
-                radiance_fraction(s, m);
-                current = mul_add(D, s.Fd, mul_add(s.Fs, Sp, current));
-            }
-            if ((m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) && --p.depth_left) {
-                float3 Fr = schlick_fresnel(clamp01(dot(s.N, s.R)), m.reflectivity);
-                next_throughput = s.refracted ? one_minus(Fr) : Fr;
-                reset(ray, hit.position, s.RF);
-                bump<COUNT>(w.bounce);
-            } else p.depth_left = 0;
-        }
-    } else {
-        p.depth_left = 0;
-        if (st.skybox_color_texture_id >= 0)
-            current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
-    }
-    add_glow(S, ray, hit.distance, current);
-    p.color = mul_add(current, p.throughput, p.color);
-    p.throughput = p.throughput * next_throughput;
-    p.o = ray.o;
-    p.d = ray.d;
-    return p.depth_left != 0;
-}
-
 // renderPixelBeauty / renderPixelDebugMode for one sample.
 template <bool COUNT>
 SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, uint32_t *stack,

@@ -1080,6 +1080,22 @@ __global__ void __launch_bounds__(128) k_finish_paths(DevScene S0, DevFrame F0, 
 }
 
 // ---- radiance-cache vertex ---------------------------------------------------
+// The network's inputs at a shaded surface: position in the scene box mapped
+// to [0,1]^3 (longest side, from the scene BVH root), roughness, ray
+// direction, shading normal, albedo x albedo map.
+SLIM_D void query_features(const DevScene &S, const Mat &m, const Ray &ray, const Surface &s, float4 f[4]) {
+    float4 r0 = make_float4(0, 0, 0, 1), r1 = make_float4(1, 1, 0, 0);
+    if (S.scene_node_count) { r0 = S.scene_nodes[0]; r1 = S.scene_nodes[1]; }
+    const float ext = fmaxf(fmaxf(r0.w - r0.x, r1.x - r0.y), r1.y - r0.z);
+    const float inv = ext > 0.0f ? 1.0f / ext : 1.0f;
+    float3 p = (s.P - f3(r0.x, r0.y, r0.z)) * inv;
+    float3 al = m.albedo * s.albedo_from_map;
+    f[0] = make_float4(p.x, p.y, p.z, m.roughness);
+    f[1] = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
+    f[2] = make_float4(s.N.x, s.N.y, s.N.z, 0.0f);
+    f[3] = make_float4(al.x, al.y, al.z, 0.0f);
+}
+
 // The path has reached the vertex the cache answers at.  Misses and emissive
 // quads finish it exactly as k_shade does; every other hit turns it into a
 // query: the segment's glow is added to the path colour now, the surface's
@@ -1110,17 +1126,7 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
             prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
             hit_distance = hit.distance;
             query = true;
-            // scene box -> [0,1]^3 (longest side), from the scene BVH root
-            float4 r0 = make_float4(0, 0, 0, 1), r1 = make_float4(1, 1, 0, 0);
-            if (S.scene_node_count) { r0 = S.scene_nodes[0]; r1 = S.scene_nodes[1]; }
-            const float ext = fmaxf(fmaxf(r0.w - r0.x, r1.x - r0.y), r1.y - r0.z);
-            const float inv = ext > 0.0f ? 1.0f / ext : 1.0f;
-            float3 p = (s.P - f3(r0.x, r0.y, r0.z)) * inv;
-            float3 al = m.albedo * s.albedo_from_map;
-            f[0] = make_float4(p.x, p.y, p.z, m.roughness);
-            f[1] = make_float4(ray.d.x, ray.d.y, ray.d.z, 0.0f);
-            f[2] = make_float4(s.N.x, s.N.y, s.N.z, 0.0f);
-            f[3] = make_float4(al.x, al.y, al.z, 0.0f);
+            query_features(S, m, ray, s, f);
         }
     } else if (st.skybox_color_texture_id >= 0) {
         current = texture_sample_cube<COUNT>(S, (uint32_t)st.skybox_color_texture_id, ray.d.x, ray.d.y, ray.d.z, w);
@@ -1326,6 +1332,81 @@ __global__ void k_cache_train_targets(const float4 *aux, const uint32_t *count, 
         float3 c = mul_add(xyz(radiance[q]), xyz(t_through[path]), xyz(t_color[path]));
         t_targets[path] = make_float4(c.x, c.y, c.z, 0.0f);
     }
+}
+
+// Self-training paths of one bounce, fused: one thread per training path
+// (queued from the cache vertex `vertex`) shades that vertex with its shadow
+// rays traced inline (the fused engine's path_segment, whose light glow the
+// frame already added), follows the bounce to the next vertex and there
+// either finishes the path into its target (miss, emissive quad) or queues
+// it as a self-training query (colour and throughput kept in t_color /
+// t_through for k_cache_train_targets).  The same arithmetic as the two
+// wavefront rounds it replaces, in a single launch of few warps: the
+// training's latency-bound tail competes less with the next frame's rays.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_train_paths(DevScene S, DevFrame F, const float4 *rays,
+                                                     const uint32_t *count, float4 *t_color, float4 *t_through,
+                                                     float4 *t_targets, CacheArgs SC, uint32_t vertex,
+                                                     unsigned long long *counters) {
+    const uint32_t n = *count;
+    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
+    uint32_t err = 0;
+    Work w = {};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounds = (n + stride - 1) / stride;
+    for (uint32_t r = 0, j = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, j += stride) {
+        bool query = false;
+        float4 feat[4];
+        PathState p;
+        uint32_t pid = 0;
+        if (j < n) {
+            const float4 a = rays[2 * (size_t)j], b = rays[2 * (size_t)j + 1];
+            pid = __float_as_uint(b.w);
+            p.o = xyz(a);
+            p.d = xyz(b);
+            p.color = f3(0, 0, 0);
+            p.throughput = f3(1, 1, 1);
+            p.depth = INFINITY;
+            p.scaling = cone_scaling<false>(F, pid);
+            p.depth_left = F.settings.max_depth - vertex + 1;
+            if (path_segment<COUNT>(S, F, p, stack, mesh_stack, err, w, false)) {
+                Ray ray;
+                reset(ray, p.o, p.d);
+                Hit hit;
+                float3 current = f3(0, 0, 0);
+                const int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
+                float hit_distance = INFINITY;
+                if (g >= 0) {
+                    hit_distance = hit.distance;
+                    Geo geo = load_geo(S, (uint32_t)g);
+                    Mat m = load_mat(S, geo.material);
+                    if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
+                        current = m.emission;
+                    } else {
+                        Surface s;
+                        prepare_for_shading<COUNT>(S, geo, m, ray, hit, p.scaling, s, w);
+                        hit_distance = hit.distance;
+                        query_features(S, m, ray, s, feat);
+                        query = true;
+                    }
+                } else if (F.settings.skybox_color_texture_id >= 0) {
+                    current = texture_sample_cube<COUNT>(S, (uint32_t)F.settings.skybox_color_texture_id, ray.d.x,
+                                                         ray.d.y, ray.d.z, w);
+                }
+                add_glow(S, ray, hit_distance, current);
+                p.color = mul_add(current, p.throughput, p.color);
+                if (query) {
+                    t_color[j] = make_float4(p.color.x, p.color.y, p.color.z, 0.0f);
+                    t_through[j] = make_float4(p.throughput.x, p.throughput.y, p.throughput.z, 0.0f);
+                }
+            }
+            if (!query) t_targets[j] = make_float4(p.color.x, p.color.y, p.color.z, 0.0f);
+        }
+        const uint32_t q = warp_append(SC.count, query);
+        if (query) append_query(SC, q, feat, p.o, p.d, j, pid, make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0));
+    }
+    if (err) atomicOr(F.error_flags, err);
+    flush_stage<COUNT>(counters, w);
 }
 
 // Waiting paths take the cache's answer: colour += throughput * radiance,
@@ -1572,6 +1653,12 @@ CacheArgs cache_args(const CacheFrame *cache) {
     return CA;
 }
 
+// Self-training paths of one bounce as one fused launch (k_train_paths) or
+// as wavefront rounds.
+#ifndef SLIM_TRAIN_FUSED
+#define SLIM_TRAIN_FUSED 0
+#endif
+
 // The training paths queued in `in` (from the cache vertex on; A sinks
 // their radiance into the training targets): traced to max_depth, or -- with
 // a training suffix, in single-request frames -- `train_suffix` bounces on,
@@ -1596,16 +1683,29 @@ cudaError_t trace_training(const RoundLaunch &L, QueueArgs &A, const CacheArgs &
         return cudaSuccess;
     }
     const uint32_t last = K + cache->train_suffix;
-    for (uint32_t depth = K; depth < last; depth++)
-        if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) != cudaSuccess)
-            return e;
     CacheArgs SC = CA;
     SC.features = cache->s_features;
     SC.aux = cache->s_aux;
     SC.count = cache->s_count;
     SC.q_color = SC.q_through = SC.q_hit = nullptr;   // the frame's own query records stay untouched
-    if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
-    if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
+    if (SLIM_TRAIN_FUSED && cache->train_suffix == 1) {
+        // one fused launch instead of the rounds at vertex K and K + 1
+        if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
+        uint32_t g = (cache->train_capacity + 127) / 128;
+        if (g > (uint32_t)(L.sms * 4)) g = (uint32_t)(L.sms * 4);
+        k_train_paths<COUNT><<<g ? g : 1, 128, 0, L.stream>>>(*L.S, *L.F, L.B->rays[in], L.B->queue_count + in,
+                                                             cache->t_color, cache->t_through, cache->t_targets, SC, K,
+                                                             L.stage(STAGE_CACHE_TRAIN));
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    } else {
+        for (uint32_t depth = K; depth < last; depth++)
+            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) !=
+                cudaSuccess)
+                return e;
+        if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
+        if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
+    }
     if ((e = nrc::launch_infer(cache->s_features, cache->s_count, 0, cache->train_capacity, cache->s_radiance, weights,
                                L.F->error_flags, L.stream)) != cudaSuccess)
         return e;

@@ -1334,81 +1334,6 @@ __global__ void k_cache_train_targets(const float4 *aux, const uint32_t *count, 
     }
 }
 
-// Self-training paths of one bounce, fused: one thread per training path
-// (queued from the cache vertex `vertex`) shades that vertex with its shadow
-// rays traced inline (the fused engine's path_segment, whose light glow the
-// frame already added), follows the bounce to the next vertex and there
-// either finishes the path into its target (miss, emissive quad) or queues
-// it as a self-training query (colour and throughput kept in t_color /
-// t_through for k_cache_train_targets).  The same arithmetic as the two
-// wavefront rounds it replaces, in a single launch of few warps: the
-// training's latency-bound tail competes less with the next frame's rays.
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_train_paths(DevScene S, DevFrame F, const float4 *rays,
-                                                     const uint32_t *count, float4 *t_color, float4 *t_through,
-                                                     float4 *t_targets, CacheArgs SC, uint32_t vertex,
-                                                     unsigned long long *counters) {
-    const uint32_t n = *count;
-    uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
-    uint32_t err = 0;
-    Work w = {};
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t rounds = (n + stride - 1) / stride;
-    for (uint32_t r = 0, j = blockIdx.x * blockDim.x + threadIdx.x; r < rounds; r++, j += stride) {
-        bool query = false;
-        float4 feat[4];
-        PathState p;
-        uint32_t pid = 0;
-        if (j < n) {
-            const float4 a = rays[2 * (size_t)j], b = rays[2 * (size_t)j + 1];
-            pid = __float_as_uint(b.w);
-            p.o = xyz(a);
-            p.d = xyz(b);
-            p.color = f3(0, 0, 0);
-            p.throughput = f3(1, 1, 1);
-            p.depth = INFINITY;
-            p.scaling = cone_scaling<false>(F, pid);
-            p.depth_left = F.settings.max_depth - vertex + 1;
-            if (path_segment<COUNT>(S, F, p, stack, mesh_stack, err, w, false)) {
-                Ray ray;
-                reset(ray, p.o, p.d);
-                Hit hit;
-                float3 current = f3(0, 0, 0);
-                const int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
-                float hit_distance = INFINITY;
-                if (g >= 0) {
-                    hit_distance = hit.distance;
-                    Geo geo = load_geo(S, (uint32_t)g);
-                    Mat m = load_mat(S, geo.material);
-                    if ((m.flags & SLIM_MATERIAL_IS_EMISSIVE) && geo.type == SLIM_GEOMETRY_QUAD && !hit.from_behind) {
-                        current = m.emission;
-                    } else {
-                        Surface s;
-                        prepare_for_shading<COUNT>(S, geo, m, ray, hit, p.scaling, s, w);
-                        hit_distance = hit.distance;
-                        query_features(S, m, ray, s, feat);
-                        query = true;
-                    }
-                } else if (F.settings.skybox_color_texture_id >= 0) {
-                    current = texture_sample_cube<COUNT>(S, (uint32_t)F.settings.skybox_color_texture_id, ray.d.x,
-                                                         ray.d.y, ray.d.z, w);
-                }
-                add_glow(S, ray, hit_distance, current);
-                p.color = mul_add(current, p.throughput, p.color);
-                if (query) {
-                    t_color[j] = make_float4(p.color.x, p.color.y, p.color.z, 0.0f);
-                    t_through[j] = make_float4(p.throughput.x, p.throughput.y, p.throughput.z, 0.0f);
-                }
-            }
-            if (!query) t_targets[j] = make_float4(p.color.x, p.color.y, p.color.z, 0.0f);
-        }
-        const uint32_t q = warp_append(SC.count, query);
-        if (query) append_query(SC, q, feat, p.o, p.d, j, pid, make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0));
-    }
-    if (err) atomicOr(F.error_flags, err);
-    flush_stage<COUNT>(counters, w);
-}
-
 // Waiting paths take the cache's answer: colour += throughput * radiance,
 // then tone mapping and the canvas write of k_shade.
 template <bool BATCH>
@@ -1653,12 +1578,6 @@ CacheArgs cache_args(const CacheFrame *cache) {
     return CA;
 }
 
-// Self-training paths of one bounce as one fused launch (k_train_paths) or
-// as wavefront rounds.
-#ifndef SLIM_TRAIN_FUSED
-#define SLIM_TRAIN_FUSED 0
-#endif
-
 // The training paths queued in `in` (from the cache vertex on; A sinks
 // their radiance into the training targets): traced to max_depth, or -- with
 // a training suffix, in single-request frames -- `train_suffix` bounces on,
@@ -1688,24 +1607,11 @@ cudaError_t trace_training(const RoundLaunch &L, QueueArgs &A, const CacheArgs &
     SC.aux = cache->s_aux;
     SC.count = cache->s_count;
     SC.q_color = SC.q_through = SC.q_hit = nullptr;   // the frame's own query records stay untouched
-    if (SLIM_TRAIN_FUSED && cache->train_suffix == 1) {
-        // one fused launch instead of the rounds at vertex K and K + 1
-        if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
-        uint32_t g = (cache->train_capacity + 127) / 128;
-        if (g > (uint32_t)(L.sms * 4)) g = (uint32_t)(L.sms * 4);
-        k_train_paths<COUNT><<<g ? g : 1, 128, 0, L.stream>>>(*L.S, *L.F, L.B->rays[in], L.B->queue_count + in,
-                                                             cache->t_color, cache->t_through, cache->t_targets, SC, K,
-                                                             L.stage(STAGE_CACHE_TRAIN));
-        count_launch();
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    } else {
-        for (uint32_t depth = K; depth < last; depth++)
-            if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) !=
-                cudaSuccess)
-                return e;
-        if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
-        if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
-    }
+    for (uint32_t depth = K; depth < last; depth++)
+        if ((e = trace_round<COUNT, BATCH>(L, A, CA, in, depth, false, false, hits_given && depth == K)) != cudaSuccess)
+            return e;
+    if ((e = cudaMemsetAsync(cache->s_count, 0, sizeof(uint32_t), L.stream)) != cudaSuccess) return e;
+    if ((e = trace_round<COUNT, BATCH>(L, A, SC, in, last, false, true)) != cudaSuccess) return e;
     if ((e = nrc::launch_infer(cache->s_features, cache->s_count, 0, cache->train_capacity, cache->s_radiance, weights,
                                L.F->error_flags, L.stream)) != cudaSuccess)
         return e;

@@ -249,3 +249,24 @@ def test_config4_plain_depth8_full_size(config2_workload):
     assert_pixels_close(pix, opix, w.width, w.height)
     assert_depths_close(dep, odep)
     assert_float_pixels_close(pix, opix)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("antialias", [L.AA_MSAA, L.AA_SSAA])
+def test_config1_full_size_antialiased(engine, antialias):
+    """Config 1 at 640x360 with the canvas's MSAA (depths for four samples
+    per pixel, draw/canvas.h:128-185) and SSAA (four samples per pixel,
+    renderer_GPU.h:23-25) layouts, against the oracle."""
+    native.set_render_options(engine=engine)
+    w = scenes.config1(0)
+    r = renderer_for(w)
+    pix, dep = r.render(Viewport(w.camera, w.width, w.height, antialias))
+    ssaa = antialias == L.AA_SSAA
+    proj = w.camera.projection(w.width, w.height, ssaa)
+    opix, odep, _ = O.oracle_render(w.scene, proj, w.settings, w.width, w.height, antialias=antialias, layout=L,
+                                    threads=0)
+    s = 2 if ssaa else 1
+    assert_pixels_close(pix, opix, s * w.width, s * w.height)
+    assert_depths_close(dep, odep)
+    assert_float_pixels_close(pix, opix)
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)

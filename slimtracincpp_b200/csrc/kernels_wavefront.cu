@@ -495,6 +495,12 @@ SLIM_D bool leaf_round(bool waiting, bool can_step) {
 // (config 2: 1.61 -> 1.57 ms with the closest-hit pass, 1.59 with the any-hit
 // pass alone).
 constexpr int kMeshBlock = 128;
+#ifndef SLIM_SHADOW_MESH_BLOCKS
+#define SLIM_SHADOW_MESH_BLOCKS 9
+#endif
+#ifndef SLIM_EXTEND_MESH_BLOCKS
+#define SLIM_EXTEND_MESH_BLOCKS 7
+#endif
 
 // Drain phase of the persistent any-hit kernel.  Once the pair queue is
 // empty, a lane with nothing left to walk takes the deepest pending subtree
@@ -547,7 +553,7 @@ SLIM_D bool push_entry(uint32_t *stack, uint32_t &bottom, uint32_t &top, uint32_
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(kMeshBlock, 9) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(kMeshBlock, SLIM_SHADOW_MESH_BLOCKS) k_shadow_mesh(DevScene S, DevFrame F, QueueArgs A) {
     const uint32_t n = *A.pair_count < A.pair_capacity ? *A.pair_count : A.pair_capacity;
     uint32_t stack[kStackCapacity];
     uint32_t err = 0;
@@ -844,7 +850,7 @@ __global__ void __launch_bounds__(256) k_extend_overflow(DevScene S0, DevFrame F
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(kMeshBlock, 7) k_extend_mesh(DevScene S, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(kMeshBlock, SLIM_EXTEND_MESH_BLOCKS) k_extend_mesh(DevScene S, DevFrame F, QueueArgs A) {
     const uint32_t cap = A.pair_capacity * 3u / 4u;
     const uint32_t n = *A.pair_count < cap ? *A.pair_count : cap;
     uint32_t stack[kStackCapacity];

@@ -205,8 +205,11 @@ typedef struct {
                                 band's launch tails overlap the other's work; into a pinned
                                 host canvas each band downloads while the next renders.
                                 0 = default (2 from 512x512 samples up, else 1), 1 = whole
-                                frame, at most 64.  Radiance-cache frames and the fused
-                                engine use one band.  The pixels are the same either way. */
+                                frame, at most 64.  The fused engine, and radiance-cache
+                                frames other than ON with overlapped training, use one
+                                band; banded cache frames gather every band's queries and
+                                answer them in one cache phase.  Plain frames' pixels are
+                                the same for any band count. */
 } SlimRenderOptions;
 enum { SLIM_CACHE_OFF = 0, SLIM_CACHE_ON = 1, SLIM_CACHE_TRUNCATE = 2, SLIM_CACHE_EXACT = 3 };
 

@@ -493,7 +493,9 @@ SLIM_D bool leaf_round(bool waiting, bool can_step) {
 // registers, 32 -> 36 warps per SM; closest hit: 73 -> 70 registers, 24 -> 28
 // warps): their walks wait on dependent loads, so warps beat registers
 // (config 2: 1.61 -> 1.57 ms with the closest-hit pass, 1.59 with the any-hit
-// pass alone).
+// pass alone).  With the later walk changes, config 2 at 9 / 7 blocks takes
+// 1.437-1.443 ms; 10 or 12 any-hit blocks 1.54 / 1.68 ms (spills), 8 or 9
+// closest-hit blocks 1.48-1.49 ms.
 constexpr int kMeshBlock = 128;
 #ifndef SLIM_SHADOW_MESH_BLOCKS
 #define SLIM_SHADOW_MESH_BLOCKS 9

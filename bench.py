@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--train-suffix", type=int, default=0,
                    help="radiance cache (config4): 0 = training paths traced to full depth (as specified); k = "
                         "traced k bounces past the cache vertex into the cache's own answer")
+    p.add_argument("--cache-scene", default="config2", choices=["config2", "config3"],
+                   help="radiance cache (config4): the scene at depth 8 -- config 2's mesh PBR scene (as "
+                        "specified) or config 3's glass/mirror/texture/IBL scene")
     p.add_argument("--no-cache-block", action="store_true",
                    help="default workload: skip the radiance-cache comparison block")
     p.add_argument("--no-batch-block", action="store_true",
@@ -523,7 +526,9 @@ def cache_comparison(torch, native, w, dev, steps, warmup, train_samples, suffix
     from slimtracincpp_b200.radiance_cache import RadianceCache
     from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport
     lib = native.lib()
-    r = RayTracingRenderer(w.scene, 8)
+    st = w.settings
+    r = RayTracingRenderer(w.scene, 8, int(st["skybox_color_texture_id"]), int(st["skybox_radiance_texture_id"]),
+                           int(st["skybox_irradiance_texture_id"]))
     vp = Viewport(w.camera, w.width, w.height)
     n = w.samples
     stream = torch.cuda.current_stream(dev)
@@ -611,7 +616,11 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     from slimtracincpp_b200 import native, scenes
     from slimtracincpp_b200.radiance_cache import RadianceCache
     from slimtracincpp_b200.renderer import RayTracingRenderer, make_canvas
-    w = scenes.config4(args.seed)
+    if args.cache_scene == "config3":
+        w = scenes.config3(args.seed, max_depth=8)
+        w.name = f"config4_cache_on_config3_glass_mirror_ibl_{w.width}x{w.height}_d8_cache2"
+    else:
+        w = scenes.config4(args.seed)
     lib = native.lib()
     n = w.samples
     steps = args.steps
@@ -627,7 +636,9 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     c = cmp["cache"][0]
 
     # end to end through the C ABI with host buffers, cache on
-    r = RayTracingRenderer(w.scene, 8)
+    st = w.settings
+    r = RayTracingRenderer(w.scene, 8, int(st["skybox_color_texture_id"]), int(st["skybox_radiance_texture_id"]),
+                           int(st["skybox_irradiance_texture_id"]))
     RadianceCache.configure(cache_depth=2, train_samples=args.train_samples, batch=16384, seed=args.seed,
                             train_suffix=args.train_suffix)
     native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
@@ -652,7 +663,7 @@ def run_cache_bench(args, torch, dist, dev, rank, world, local):
     value = whole_job_rate(c["rays_per_frame"], steps, world, cache_total)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": cache_total / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": "synthetic (seeded config2 scene, depth 8)",
+            "dtype": "f32 trace, bf16 MLP (f32 accumulate)", "data": f"synthetic (seeded {args.cache_scene} scene, depth 8)",
             "config": {"workload": w.name, "width": w.width, "height": w.height, "max_depth": 8, "cache_depth": 2,
                        "train_samples_per_frame": args.train_samples, "train_suffix": args.train_suffix,
                        "batch": 16384, "learning_rate": 1e-2, "cache_warmup_frames": c["cache_warmup_frames"],

@@ -427,6 +427,25 @@ int slimRadianceCacheSetWeights(const float *params, uint32_t count);
 int slimRadianceCacheGetWeights(float *params, uint32_t count);
 /* Mean-loss gradient of the last training step. */
 int slimRadianceCacheGetGradients(float *grad, uint32_t count);
+
+/* Training checkpoint: what online training continues from.  A state of
+ * SLIM_NRC_STATE_BYTES is this header, then the f32 master weights, Adam's
+ * first moments and Adam's second moments, SLIM_NRC_PARAMS floats each.
+ * Save waits for training in flight.  Load (needs slimInitDataOnGPU)
+ * configures the cache from the header's config, then restores the weights,
+ * the moments and both counters, so the next step and the next frame's
+ * training-set selection continue as if training had never stopped. */
+#define SLIM_NRC_STATE_MAGIC 0x4B43524Eu
+typedef struct {
+    uint32_t magic;          /* SLIM_NRC_STATE_MAGIC */
+    uint32_t params;         /* SLIM_NRC_PARAMS */
+    uint32_t steps;          /* Adam steps taken (the bias corrections' exponent) */
+    uint32_t frames;         /* cache frames rendered (offsets the training-set selection) */
+    SlimRadianceCacheConfig config;
+} SlimRadianceCacheStateHeader;
+#define SLIM_NRC_STATE_BYTES (sizeof(SlimRadianceCacheStateHeader) + 3u * SLIM_NRC_PARAMS * sizeof(float))
+int slimRadianceCacheSaveState(void *state, uint64_t bytes);
+int slimRadianceCacheLoadState(const void *state, uint64_t bytes);
 /* Device pointers: radiance (float4 per sample, rgb) of `count` samples of
  * SLIM_NRC_FEATURES floats.  Asynchronous on `stream`. */
 int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radiance, void *stream);
@@ -486,6 +505,7 @@ int slimBatchGetPlan(SlimBatchPlan *plan);
 int slimBatchRender(void *stream);
 
 SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheConfig) == 48, "RadianceCacheConfig is 48 bytes");
+SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheStateHeader) == 64, "RadianceCacheStateHeader is 64 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRadianceCacheStats) == 32, "RadianceCacheStats is 32 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimRenderRequest) == 184, "RenderRequest is 184 bytes");
 SLIM_STATIC_ASSERT(sizeof(SlimBatchPlan) == 40, "BatchPlan is 40 bytes");

@@ -1594,16 +1594,9 @@ int upload_cache_weights(Context &c, const float *params) {
     return cache_sync_errors(c);
 }
 
-}  // namespace
-
-extern "C" {
-
-int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    Context &c = g_ctx;
-    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
-    if (!config) return set_error(SLIM_ERR_ARGUMENT, "config is null");
-    const SlimRadianceCacheConfig &k = *config;
+// Validates `k`, allocates the cache's buffers, uploads `weights` and clears
+// the Adam state and both counters.
+int configure_cache(Context &c, const SlimRadianceCacheConfig &k, const float *weights) {
     if (k.cache_depth < 2 || k.cache_depth > 255 || !k.batch || !(k.learning_rate > 0.0f) || !(k.beta1 >= 0.0f) ||
         !(k.beta1 < 1.0f) || !(k.beta2 >= 0.0f) || !(k.beta2 < 1.0f) || !(k.epsilon > 0.0f) ||
         k.train_samples > (1u << 26) || k.train_suffix > 255)
@@ -1627,11 +1620,23 @@ int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
     st.config = k;
     st.error_flags = c.d_error.ptr;
     SLIM_CUDA(nrc::prepare(), "radiance cache kernel attributes");
-    std::vector<float> w;
-    init_cache_weights(k.seed, w);
-    if ((rc = upload_cache_weights(c, w.data()))) return rc;
+    if ((rc = upload_cache_weights(c, weights))) return rc;
     st.configured = true;
     return SLIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int slimRadianceCacheConfigure(const SlimRadianceCacheConfig *config) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!config) return set_error(SLIM_ERR_ARGUMENT, "config is null");
+    std::vector<float> w;
+    init_cache_weights(config->seed, w);
+    return configure_cache(c, *config, w.data());
 }
 
 int slimRadianceCacheGetConfig(SlimRadianceCacheConfig *config) {
@@ -1670,6 +1675,54 @@ int slimRadianceCacheGetGradients(float *grad, uint32_t count) {
     if (rc) return rc;
     SLIM_CUDA(cudaMemcpy(grad, c.cache.grad.ptr, nrc::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read gradient");
     return SLIM_OK;
+}
+
+int slimRadianceCacheSaveState(void *state, uint64_t bytes) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.cache.configured) return set_error(SLIM_ERR_STATE, "radiance cache not configured");
+    if (!state || bytes < SLIM_NRC_STATE_BYTES) return set_error(SLIM_ERR_ARGUMENT, "state needs SLIM_NRC_STATE_BYTES");
+    int rc = cache_sync_errors(c);
+    if (rc) return rc;
+    const Context::Cache &k = c.cache;
+    SlimRadianceCacheStateHeader h{};
+    uint32_t counters[2] = {0, 0};
+    SLIM_CUDA(cudaMemcpy(counters, k.state.ptr, sizeof(counters), cudaMemcpyDeviceToHost), "read cache counters");
+    h.magic = SLIM_NRC_STATE_MAGIC;
+    h.params = (uint32_t)nrc::kParams;
+    h.steps = counters[0];
+    h.frames = counters[1];
+    h.config = k.config;
+    uint8_t *out = (uint8_t *)state;
+    memcpy(out, &h, sizeof(h));
+    float *f = (float *)(out + sizeof(h));
+    const size_t n = (size_t)nrc::kParams * sizeof(float);
+    SLIM_CUDA(cudaMemcpy(f, k.params.ptr, n, cudaMemcpyDeviceToHost), "read weights");
+    SLIM_CUDA(cudaMemcpy(f + nrc::kParams, k.m.ptr, n, cudaMemcpyDeviceToHost), "read adam moments");
+    SLIM_CUDA(cudaMemcpy(f + 2 * nrc::kParams, k.v.ptr, n, cudaMemcpyDeviceToHost), "read adam moments");
+    return SLIM_OK;
+}
+
+int slimRadianceCacheLoadState(const void *state, uint64_t bytes) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    Context &c = g_ctx;
+    if (!c.initialized) return set_error(SLIM_ERR_STATE, "slimInitDataOnGPU has not been called");
+    if (!state || bytes < SLIM_NRC_STATE_BYTES) return set_error(SLIM_ERR_ARGUMENT, "state needs SLIM_NRC_STATE_BYTES");
+    SlimRadianceCacheStateHeader h;
+    memcpy(&h, state, sizeof(h));
+    if (h.magic != SLIM_NRC_STATE_MAGIC || h.params != (uint32_t)nrc::kParams)
+        return set_error(SLIM_ERR_ARGUMENT, "not a radiance cache state of this network");
+    std::vector<float> f((size_t)3 * nrc::kParams);
+    memcpy(f.data(), (const uint8_t *)state + sizeof(h), f.size() * sizeof(float));
+    int rc = configure_cache(c, h.config, f.data());
+    if (rc) return rc;
+    const Context::Cache &k = c.cache;
+    const size_t n = (size_t)nrc::kParams * sizeof(float);
+    const uint32_t counters[2] = {h.steps, h.frames};
+    SLIM_CUDA(cudaMemcpy(k.m.ptr, f.data() + nrc::kParams, n, cudaMemcpyHostToDevice), "restore adam moments");
+    SLIM_CUDA(cudaMemcpy(k.v.ptr, f.data() + 2 * nrc::kParams, n, cudaMemcpyHostToDevice), "restore adam moments");
+    SLIM_CUDA(cudaMemcpy(k.state.ptr, counters, sizeof(counters), cudaMemcpyHostToDevice), "restore cache counters");
+    return cache_sync_errors(c);
 }
 
 int slimRadianceCacheQuery(const void *d_features, uint32_t count, void *d_radiance, void *stream) {

@@ -101,6 +101,8 @@ RENDER_OPTIONS = _dt([("engine", i4, 0), ("ray_cones", i4, 4), ("scene_bvh", i4,
 CACHE_CONFIG = _dt([("cache_depth", u4, 0), ("train_samples", u4, 4), ("batch", u4, 8), ("seed", u4, 12),
                     ("learning_rate", f4, 16), ("beta1", f4, 20), ("beta2", f4, 24), ("epsilon", f4, 28),
                     ("train", u4, 32), ("overlap", u4, 36), ("train_suffix", u4, 40), ("_reserved", u4, 44)], 48)
+CACHE_STATE_HEADER = _dt([("magic", u4, 0), ("params", u4, 4), ("steps", u4, 8), ("frames", u4, 12),
+                          ("config", CACHE_CONFIG, 16)], 64)
 CACHE_STATS = _dt([("frames", u8, 0), ("steps", u8, 8), ("queries", u4, 16), ("train_samples", u4, 20),
                    ("loss", f4, 24), ("_pad", f4, 28)], 32)
 CACHE_OFF, CACHE_ON, CACHE_TRUNCATE, CACHE_EXACT = 0, 1, 2, 3
@@ -113,6 +115,8 @@ BATCH_PLAN = _dt([("queue_capacity", u4, 0), ("tile_pixels", u4, 4), ("block_siz
                   ("batch_ms", f4, 16), ("candidates", u4, 20), ("graph_nodes", u4, 24), ("tuned", u4, 28),
                   ("persistent", u4, 32), ("_pad", u4, 36)], 40)
 NRC_PARAMS = 18624
+NRC_STATE_MAGIC = 0x4B43524E
+NRC_STATE_BYTES = 64 + 3 * NRC_PARAMS * 4
 NRC_FEATURES = 16
 WORK_COUNTERS = _dt([(n, u8, 8 * i) for i, n in enumerate(
     ["primary_rays", "shadow_rays", "bounce_rays", "scene_node_tests", "mesh_node_tests", "triangle_tests",

@@ -29,7 +29,8 @@ EXPORTS = [
     "slimGetStageStats", "slimResetStageStats", "slimRenderToDeviceNoAlloc",
     "slimRadianceCacheConfigure", "slimRadianceCacheGetConfig", "slimRadianceCacheSetWeights",
     "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients", "slimRadianceCacheQuery",
-    "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimSynchronize",
+    "slimRadianceCacheTrain", "slimRadianceCacheGetStats", "slimRadianceCacheJoin", "slimRadianceCacheSaveState",
+    "slimRadianceCacheLoadState", "slimSynchronize",
     "slimGetLaunchCount", "slimPick", "slimDownloadSceneBVH", "slimSaveScene", "slimReadSceneHeader", "slimLoadScene",
     "slimBatchSetRequests", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender",
 ]
@@ -86,6 +87,8 @@ def lib():
     for name in ["slimRadianceCacheSetWeights", "slimRadianceCacheGetWeights", "slimRadianceCacheGetGradients"]:
         getattr(h, name).argtypes = [P, C.c_uint32]
     h.slimRadianceCacheQuery.argtypes = [P, C.c_uint32, P, P]
+    h.slimRadianceCacheSaveState.argtypes = [P, C.c_uint64]
+    h.slimRadianceCacheLoadState.argtypes = [P, C.c_uint64]
     for name in ["slimSynchronize", "slimRadianceCacheJoin", "slimGetLaunchCount", "slimBatchTune", "slimBatchSetPlan", "slimBatchGetPlan", "slimBatchRender"]:
         getattr(h, name).argtypes = [P]
     h.slimBatchSetRequests.argtypes = [P, C.c_uint32]

@@ -47,6 +47,29 @@ class RadianceCache:
         w = np.ascontiguousarray(w, np.float32)
         check(lib().slimRadianceCacheSetWeights(ptr(w), len(w)))
 
+    def save_state(self) -> bytes:
+        """Checkpoint: header (magic, params, Adam steps, cache frames,
+        config), then weights, first and second Adam moments."""
+        buf = np.zeros(L.NRC_STATE_BYTES, np.uint8)
+        check(lib().slimRadianceCacheSaveState(ptr(buf), buf.nbytes))
+        return buf.tobytes()
+
+    @staticmethod
+    def load_state(state: bytes) -> "RadianceCache":
+        """Configures the cache from a checkpoint and resumes its training."""
+        buf = np.frombuffer(bytes(state), np.uint8).copy()
+        check(lib().slimRadianceCacheLoadState(ptr(buf), buf.nbytes))
+        return RadianceCache()
+
+    @staticmethod
+    def parse_state(state: bytes):
+        """(header record, weights, first moments, second moments) of a checkpoint."""
+        buf = np.frombuffer(bytes(state), np.uint8)
+        h = buf[:L.CACHE_STATE_HEADER.itemsize].view(L.CACHE_STATE_HEADER)[0]
+        f = buf[L.CACHE_STATE_HEADER.itemsize:L.NRC_STATE_BYTES].view(np.float32)
+        n = L.NRC_PARAMS
+        return h, f[:n], f[n:2 * n], f[2 * n:3 * n]
+
     def gradients(self):
         g = np.zeros(L.NRC_PARAMS, np.float32)
         check(lib().slimRadianceCacheGetGradients(ptr(g), L.NRC_PARAMS))

@@ -276,3 +276,59 @@ def test_banded_cache_frames_gather_every_band():
     # weights) differ: both must still be well trained
     pa, pb = psnr(to8(a, w.width, w.height), ref), psnr(to8(b, w.width, w.height), ref)
     assert min(pa, pb) > 40.0, (pa, pb)
+
+
+def test_checkpoint_resumes_training_exactly(cache):
+    """slimRadianceCacheSaveState / LoadState: training continued from a
+    restored checkpoint takes the same Adam steps, bit for bit, as training
+    that never stopped; restoring the weights alone (moments cleared) does
+    not."""
+    rng = np.random.default_rng(11)
+    c = RadianceCache.configure(seed=3, batch=4096, learning_rate=5e-3, train=False)
+    f = [gpu(rand_features(rng, 4096)) for _ in range(5)]
+    t = [gpu(rng.uniform(0, 2, (4096, 4)).astype(np.float32)) for _ in range(5)]
+    for i in range(3):
+        c.train(f[i].data_ptr(), t[i].data_ptr(), 4096)
+    state = c.save_state()
+    assert len(state) == L.NRC_STATE_BYTES
+    h, w, m, v = RadianceCache.parse_state(state)
+    assert h["magic"] == L.NRC_STATE_MAGIC and h["params"] == L.NRC_PARAMS and h["steps"] == 3
+    assert h["config"]["seed"] == 3 and h["config"]["batch"] == 4096 and h["config"]["train"] == 0
+    assert np.array_equal(w, c.weights) and np.any(m != 0) and np.all(v >= 0) and np.any(v > 0)
+
+    def two_more_steps(cc):
+        for i in (3, 4):
+            cc.train(f[i].data_ptr(), t[i].data_ptr(), 4096)
+        return cc.weights
+
+    resumed_without_stop = two_more_steps(c)
+    c2 = RadianceCache.load_state(state)
+    assert c2.stats()["steps"] == 3 and np.array_equal(c2.weights, w)
+    assert c2.config()["learning_rate"] == np.float32(5e-3)
+    assert np.array_equal(two_more_steps(c2), resumed_without_stop)
+    c2.weights = w                          # same weights, Adam state cleared
+    assert not np.array_equal(two_more_steps(c2), resumed_without_stop)
+
+
+def test_checkpoint_keeps_the_frame_counter():
+    """Online training picks each frame's training set from the cache-frame
+    counter; a restored checkpoint continues the count."""
+    w = scenes.small_textured_scene(1, 64, 36, max_depth=4)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    c = RadianceCache.configure(cache_depth=2, train_samples=1024, batch=256, seed=2, train_suffix=1, overlap=False)
+    try:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, radiance_cache=L.CACHE_ON)
+        for _ in range(3):
+            r.render(vp, update_scene=False)
+        s = c.stats()
+        state = c.save_state()
+        assert s["frames"] == 3 and s["steps"] > 0
+        r.render(vp, update_scene=False)
+        c2 = RadianceCache.load_state(state)
+        assert c2.stats()["frames"] == 3 and c2.stats()["steps"] == s["steps"]
+        assert c2.config()["train_suffix"] == 1 and c2.config()["overlap"] == 0
+        img, _ = r.render(vp, update_scene=False)
+        assert c2.stats()["frames"] == 4 and np.isfinite(img).all()
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)

@@ -43,6 +43,20 @@ def test_cuda_calls_fail_loudly_without_gpu_or_init():
     assert lib.slimGetLastError()
 
 
+def test_cache_checkpoint_layout_and_refusals():
+    """The checkpoint header and size agree with the C header; without a
+    configured cache (or slimInitDataOnGPU) both calls refuse with STATE and
+    touch no device."""
+    text = HEADER.read_text()
+    assert int(re.search(r"#define SLIM_NRC_STATE_MAGIC (0x[0-9A-Fa-f]+)u", text).group(1), 16) == L.NRC_STATE_MAGIC
+    assert L.CACHE_STATE_HEADER.itemsize == 64 and L.CACHE_STATE_HEADER.fields["config"][1] == 16
+    assert L.NRC_STATE_BYTES == 64 + 3 * 4 * L.NRC_PARAMS
+    lib = native.lib()
+    buf = np.zeros(L.NRC_STATE_BYTES, np.uint8)
+    assert lib.slimRadianceCacheSaveState(native.ptr(buf), buf.nbytes) == 3
+    assert lib.slimRadianceCacheLoadState(native.ptr(buf), buf.nbytes) == 3
+
+
 def test_render_options_are_validated():
     """Options outside their ranges are refused without touching the device."""
     for bad in ({"row_bands": -1}, {"row_bands": 65}, {"block_size": 48}, {"radiance_cache": 4}):

@@ -895,7 +895,10 @@ int read_counters(Context &c, cudaStream_t stream) {
 // are in flight at once and the ends of one band's persistent launches, where most of the GPU
 // waits on a few long walks, overlap the other band's work.  Into a pinned
 // host canvas every band downloads as soon as it is done, while the next
-// renders.  The pixels are the same for any band count.
+// renders.  The pixels are the same for any band count.  Two bands, one
+// per lane (config 2: 1.44 ms, 1.79 end to end); three, four or six bands
+// queue behind each other on the two lanes: 1.82 / 1.79 / 1.95 ms (2.08 /
+// 2.19 / 2.25 end to end).
 constexpr uint32_t kDefaultRowBands = 2;
 constexpr size_t kStagedDownloadBytes = 4u << 20;   // pageable canvases from here up go through staging
 constexpr double kBandRatio = 2.0 / 3.0;

@@ -40,7 +40,7 @@ struct WavefrontBuffers {
     float4 *path_throughput;         // per sample: throughput (xyz)
     float4 *rays[2];                 // ping-pong ray queues, 2 float4 per ray
     uint32_t *queue_count;           // [0..1] ray queues, [2] shadow queue, [3] pairs, [4] pair cursor (8 slots)
-    float4 *hits;                    // 3 float4 per queue slot
+    float4 *hits;                    // hit records: three planes of `capacity` float4
     float4 *shadow_rays;             // 2 float4 per shadow ray
     unsigned long long *shadow_mask; // per queue slot: occluded-light bits
     float4 *pairs;                   // shadow ray x mesh instance candidates, 3 float4 each

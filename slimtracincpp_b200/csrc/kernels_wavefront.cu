@@ -52,21 +52,31 @@ SLIM_D uint32_t warp_append(uint32_t *counter, bool want) {
     return base + (uint32_t)__popc(ballot & ((1u << lane_id()) - 1u));
 }
 
-SLIM_D void store_hit(float4 *hits, uint32_t slot, int g, const Hit &h) {
-    float4 *p = hits + 3 * (size_t)slot;
-    p[0] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.distance);
-    p[1] = make_float4(h.u, h.v, h.uv_coverage, h.NdotRd);
-    p[2] = make_float4(__int_as_float(g), __uint_as_float((uint32_t)h.from_behind), __uint_as_float(h.id), 0.0f);
+// Hit records in three planes of `stride` float4 (one entry per queue slot):
+//   plane 0 (normal.xyz, distance), plane 1 (u, v, uv coverage, N.Rd),
+//   plane 2 (geometry, from behind, triangle, 0).
+// A miss (geometry -1) writes and reads plane 2 only: most primary rays of
+// an open scene miss, and their records then cost one 16-byte entry in
+// the contiguous plane instead of 48 bytes.
+SLIM_D void store_hit(float4 *hits, uint32_t stride, uint32_t slot, int g, const Hit &h) {
+    hits[2 * (size_t)stride + slot] =
+        make_float4(__int_as_float(g), __uint_as_float((uint32_t)h.from_behind), __uint_as_float(h.id), 0.0f);
+    if (g < 0) return;
+    hits[slot] = make_float4(h.normal.x, h.normal.y, h.normal.z, h.distance);
+    hits[(size_t)stride + slot] = make_float4(h.u, h.v, h.uv_coverage, h.NdotRd);
 }
-SLIM_D int load_hit(const float4 *hits, uint32_t slot, Hit &h) {
-    const float4 *p = hits + 3 * (size_t)slot;
-    float4 a = p[0], b = p[1], c = p[2];
+SLIM_D int load_hit(const float4 *hits, uint32_t stride, uint32_t slot, Hit &h) {
+    const float4 c = hits[2 * (size_t)stride + slot];
+    const int g = __float_as_int(c.x);
+    h.distance = INFINITY;
+    if (g < 0) return g;
+    const float4 a = hits[slot], b = hits[(size_t)stride + slot];
     h.normal = xyz(a);
     h.distance = a.w;
     h.u = b.x; h.v = b.y; h.uv_coverage = b.z; h.NdotRd = b.w;
     h.from_behind = __float_as_uint(c.y) != 0;
     h.id = __float_as_uint(c.z);
-    return __float_as_int(c.x);
+    return g;
 }
 
 template <bool COUNT>
@@ -100,7 +110,8 @@ struct QueueArgs {
     float4 *rays_out;
     const uint32_t *count_in;     // null: count = samples
     uint32_t *count_out;
-    float4 *hits;
+    float4 *hits;                 // hit records, three planes of hit_stride entries
+    uint32_t hit_stride;
     float4 *shadow_rays;
     uint32_t *shadow_count;
     unsigned long long *masks;    // per slot: bit i = light i occluded
@@ -200,7 +211,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene S0, DevFrame F0, QueueA
         reset(ray, o, d);
         Hit hit;
         int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
-        store_hit(A.hits, slot, g, hit);
+        store_hit(A.hits, A.hit_stride, slot, g, hit);
     }
     if (err) atomicOr(F0.error_flags, err);
     flush_stage<COUNT>(A.counters, w);
@@ -231,7 +242,6 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, Qu
         bool shaded = false;
         uint32_t lights = 0, pid = 0;
         if (live) {
-            if (A.light_begin == 0) A.masks[slot] = 0ull;
             float3 o, d;
             uint32_t path;
             load_ray(F0, A, slot, o, d, path, pid);
@@ -239,7 +249,7 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, Qu
             const DevFrame &F = frame_of<BATCH>(F0, A, pid);
             lights = S.light_count;
             Hit hit;
-            int g = load_hit(A.hits, slot, hit);
+            int g = load_hit(A.hits, A.hit_stride, slot, hit);
             if (g >= 0 && !at_cache_vertex<BATCH>(F, A)) {
                 Geo geo = load_geo(S, (uint32_t)g);
                 Mat m = load_mat(S, geo.material);
@@ -248,6 +258,8 @@ __global__ void __launch_bounds__(256) k_shadow_gen(DevScene S0, DevFrame F0, Qu
                     reset(ray, scale_add(d, kTraceOffset, o), d);
                     prepare_for_shading<COUNT>(S, geo, m, ray, hit, cone_scaling<BATCH>(F, pid), s, w);
                     shaded = true;
+                    // occluded-light bits: read by shade for shaded hits only
+                    if (A.light_begin == 0) A.masks[slot] = 0ull;
                 }
             }
             if (!BATCH && A.early_depth && A.light_begin == 0) {
@@ -820,7 +832,7 @@ __global__ void __launch_bounds__(256) k_extend_scene(DevScene S0, DevFrame F0, 
             overflow[atomicAdd(A.pair_count + 2, 1u)] = slot;
         } else {
             A.masks[slot] = best_geo >= 0 ? hit_key(hit.distance, best_k) : kNoHitKey;
-            store_hit(A.hits, slot, best_geo, hit);
+            store_hit(A.hits, A.hit_stride, slot, best_geo, hit);
         }
     }
     if (err) atomicOr(F0.error_flags, err);
@@ -845,7 +857,7 @@ __global__ void __launch_bounds__(256) k_extend_overflow(DevScene S0, DevFrame F
         reset(ray, o, d);
         Hit hit;
         int g = scene_trace<COUNT>(S, ray, hit, false, INFINITY, stack, mesh_stack, err, w);
-        store_hit(A.hits, slot, g, hit);
+        store_hit(A.hits, A.hit_stride, slot, g, hit);
     }
     if (err) atomicOr(F0.error_flags, err);
     flush_stage<COUNT>(A.counters, w);
@@ -993,7 +1005,7 @@ __global__ void __launch_bounds__(256) k_extend_resolve(DevScene S0, DevFrame F0
         h.position = f3(0, 0, 0);
         mesh_hit_attributes<COUNT>(S, m, h, w);
         h.NdotRd = -(dot(h.normal, xyz(p1)));
-        store_hit(A.hits, slot, (int)__float_as_uint(p3.x), h);
+        store_hit(A.hits, A.hit_stride, slot, (int)__float_as_uint(p3.x), h);
     }
     flush_stage<COUNT>(A.counters, w);
 }
@@ -1117,7 +1129,7 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
     Ray ray;
     reset(ray, scale_add(d, kTraceOffset, o), d);
     Hit hit;
-    int g = load_hit(A.hits, slot, hit);
+    int g = load_hit(A.hits, A.hit_stride, slot, hit);
     float4 pc = A.path_color[path];
     float3 color = xyz(pc), throughput = xyz(A.path_throughput[path]);
     float3 current = f3(0, 0, 0);
@@ -1149,11 +1161,14 @@ SLIM_D bool cache_vertex(const DevScene &S, const DevFrame &F, const QueueArgs &
     return query;
 }
 
+// `hits`: the round's hit planes (stride entries each), whose record of
+// `slot` the query keeps (null: none kept).
 SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], float3 o, float3 d, uint32_t path,
-                         uint32_t pid, float4 q_color, float4 q_through, const float4 *hit = nullptr) {
-    if (C.q_hit && hit) {
+                         uint32_t pid, float4 q_color, float4 q_through, const float4 *hits = nullptr,
+                         uint32_t stride = 0, uint32_t slot = 0) {
+    if (C.q_hit && hits) {
         float4 *h = C.q_hit + 3 * (size_t)q;
-        h[0] = hit[0]; h[1] = hit[1]; h[2] = hit[2];
+        h[0] = hits[slot]; h[1] = hits[(size_t)stride + slot]; h[2] = hits[2 * (size_t)stride + slot];
     }
     float4 *p = C.features + 4 * (size_t)q;
     p[0] = f[0]; p[1] = f[1]; p[2] = f[2]; p[3] = f[3];
@@ -1194,7 +1209,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, Queu
                 Ray ray;
                 reset(ray, scale_add(d, kTraceOffset, o), d);
                 Hit hit;
-                int g = load_hit(A.hits, slot, hit);
+                int g = load_hit(A.hits, A.hit_stride, slot, hit);
                 float4 pc = A.depth == 1 ? make_float4(0, 0, 0, INFINITY) : A.path_color[path];
                 float3 color = xyz(pc), throughput = A.depth == 1 ? f3(1, 1, 1) : xyz(A.path_throughput[path]);
                 float depth = pc.w;
@@ -1285,7 +1300,7 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
             query = cache_vertex<COUNT, false>(S, F, A, slot, path, pid, o, d, feat, w, qc, qt);
         }
         uint32_t q = warp_append(C.count, query);
-        if (query) append_query(C, q, feat, o, d, path, pid, qc, qt, A.hits + 3 * (size_t)slot);
+        if (query) append_query(C, q, feat, o, d, path, pid, qc, qt, A.hits, A.hit_stride, slot);
     }
     flush_stage<COUNT>(A.counters, w);
 }
@@ -1295,7 +1310,7 @@ __global__ void __launch_bounds__(256) k_cache_gather(DevScene S, DevFrame F, Qu
 // more queries than training paths the set is stratified: j takes query
 // floor((j + u) * queries / capacity), u = frac(0.618034 * frame) (a
 // golden-ratio sequence, so consecutive frames train on different queries).
-__global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count, float4 *hits) {
+__global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count, float4 *hits, uint32_t hit_stride) {
     const uint32_t nq = *C.count, cap = C.train_capacity;
     const uint32_t n = nq < cap ? nq : cap;
     const double f = (double)*C.frame_counter * 0.6180339887498949;
@@ -1313,8 +1328,9 @@ __global__ void k_cache_select(CacheArgs C, float4 *rays, uint32_t *ray_count, f
         }
         if (C.q_hit && hits) {   // the query's hit: the training path's first round needs no extend
             const float4 *h = C.q_hit + 3 * (size_t)idx;
-            float4 *t = hits + 3 * (size_t)j;
-            t[0] = h[0]; t[1] = h[1]; t[2] = h[2];
+            hits[j] = h[0];
+            hits[(size_t)hit_stride + j] = h[1];
+            hits[2 * (size_t)hit_stride + j] = h[2];
         }
         float4 a = C.aux[2 * (size_t)idx], b = C.aux[2 * (size_t)idx + 1];
         rays[2 * (size_t)j] = make_float4(a.x, a.y, a.z, __uint_as_float(j));
@@ -1659,7 +1675,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (timer) timer->begin(STAGE_CACHE, stream);
         uint32_t g = (cache->train_capacity + 255) / 256;
         if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
-        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, TB.rays[0], TB.queue_count, TB.hits);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, TB.rays[0], TB.queue_count, TB.hits, TB.capacity);
         count_launch();
         if (timer) timer->end(STAGE_CACHE, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1668,6 +1684,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         RoundLaunch TL{L.S, L.F, &TB, L.block, L.sms, ts, nullptr, nullptr, TB.capacity, L.lights, L.split_extend};
         QueueArgs TA = A;
         TA.hits = TB.hits;
+        TA.hit_stride = TB.capacity;
         TA.shadow_rays = TB.shadow_rays;
         TA.masks = TB.shadow_mask;
         TA.pairs = TB.pairs;
@@ -1692,7 +1709,7 @@ cudaError_t cache_phase(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
         if (timer) timer->begin(STAGE_CACHE, stream);
         uint32_t g = (cache->train_capacity + 255) / 256;
         if (g > (uint32_t)(L.sms * 8)) g = (uint32_t)(L.sms * 8);
-        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in, B.hits);
+        k_cache_select<<<g ? g : 1, 256, 0, stream>>>(CA, B.rays[in], B.queue_count + in, B.hits, B.capacity);
         count_launch();
         if (timer) timer->end(STAGE_CACHE, stream);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1748,6 +1765,7 @@ cudaError_t run_frame(const DevScene &S, const DevFrame &F, const WavefrontBuffe
     if (e != cudaSuccess) return e;
     QueueArgs A{};
     A.hits = B.hits;
+    A.hit_stride = B.capacity;
     A.shadow_rays = B.shadow_rays;
     A.masks = B.shadow_mask;
     A.pairs = B.pairs;
@@ -1854,6 +1872,7 @@ cudaError_t run_batch(const BatchFrame &BF, const WavefrontBuffers &B0, int bloc
             return e;
         QueueArgs A{};
         A.hits = B.hits;
+        A.hit_stride = B.capacity;
         A.shadow_rays = B.shadow_rays;
         A.masks = B.shadow_mask;
         A.pairs = B.pairs;

@@ -368,9 +368,14 @@ SLIM_D bool shadow_leaf(const DevScene &S, const QueueArgs &A, uint32_t tag, uin
 }
 
 // Capped at 64 registers (4 blocks per SM instead of 3): latency-bound, the
-// extra warps pay for the few spills (config 2: shadow 0.157 -> 0.149 ms).
+// extra warps pay for the few spills (config 2: shadow 0.157 -> 0.149 ms;
+// re-measured on the final build, 3 blocks at 78 registers without spills:
+// 0.155 against 0.148 ms).
+#ifndef SLIM_SHADOW_SCENE_BLOCKS
+#define SLIM_SHADOW_SCENE_BLOCKS 4
+#endif
 template <bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256, 4) k_shadow_scene(DevScene S0, DevFrame F, QueueArgs A) {
+__global__ void __launch_bounds__(256, SLIM_SHADOW_SCENE_BLOCKS) k_shadow_scene(DevScene S0, DevFrame F, QueueArgs A) {
     uint32_t n = *A.shadow_count;
     uint32_t stack[kStackCapacity], mesh_stack[kStackCapacity];
     uint32_t err = 0;
@@ -1182,9 +1187,15 @@ SLIM_D void append_query(const CacheArgs &C, uint32_t q, const float4 f[4], floa
 
 // ---- shade: colour of this segment, next bounce, finished paths --------
 // Capped at 80 registers (3 blocks per SM instead of 2): latency-bound, the
-// extra warps pay for the spills (config 2: shade 0.180 -> 0.173 ms).
+// extra warps pay for the spills (config 2: shade 0.180 -> 0.173 ms).  The
+// spills are real traffic -- in round 1, 340 MB of local stores reach L2
+// (ncu) -- but on the final build 2 blocks at 128 registers, without
+// spills, measure the same (0.183 against 0.182 ms).
+#ifndef SLIM_SHADE_BLOCKS
+#define SLIM_SHADE_BLOCKS 3
+#endif
 template <bool COUNT, bool BATCH>
-__global__ void __launch_bounds__(256, 3) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
+__global__ void __launch_bounds__(256, SLIM_SHADE_BLOCKS) k_shade(DevScene S0, DevFrame F0, QueueArgs A) {
     uint32_t n = queue_size(A);
     if (A.slot_end && A.slot_end < n) n = A.slot_end;
     const uint32_t first = A.slot_begin;

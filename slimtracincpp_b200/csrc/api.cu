@@ -821,8 +821,13 @@ int ensure_wavefront(Context &c, uint32_t samples, int set) {
     size_t max_pairs = budget / (3 * sizeof(float4));
     if (pairs > max_pairs) pairs = max_pairs;
     if (pairs > 0xFFFFFFFFull) pairs = 0xFFFFFFFFull;
-    if (W.B.capacity >= samples && W.B.shadow_capacity >= shadow && W.B.pair_capacity >= pairs)
+    if (W.B.capacity >= samples && W.shadow_rays.count >= 2 * shadow && W.pairs.count >= 3 * (pairs ? pairs : 1)) {
+        // the arrays are large enough; this frame's queue budget still sets
+        // the capacities (overflow and light batches as a fresh context's)
+        W.B.shadow_capacity = (uint32_t)shadow;
+        W.B.pair_capacity = (uint32_t)pairs;
         return SLIM_OK;
+    }
     uint32_t n = samples;
     int rc = 0;
     if ((rc = W.color.reserve(n, "alloc path colour"))) return rc;

@@ -270,3 +270,36 @@ def test_config1_full_size_antialiased(engine, antialias):
     assert_depths_close(dep, odep)
     assert_float_pixels_close(pix, opix)
     native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+
+
+def test_queue_overflow_and_light_batches_match_oracle():
+    """Config 2's scene at 640x360 with a 1 MiB queue budget: the shadow queue
+    holds one ray per sample, so the 4 lights go in 4 batches; the candidate
+    queue holds 21,845 pairs (closest-hit candidates stop at three quarters of
+    that), far fewer than the primary rays that reach a mesh instance, so
+    most rays are traced whole by k_extend_overflow and the shadow rays whose
+    pairs do not fit walk their instances inline.  The frame is bit-identical
+    to the one with the default budget and matches the oracle."""
+    w = scenes.config2(0, 640, 360)
+    r = renderer_for(w)
+    vp = Viewport(w.camera, w.width, w.height)
+    def shadow_launches():
+        return {s["name"]: s["launches"] for s in native.stage_stats()}["shadow"]
+
+    try:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, row_bands=1, profile_stages=True)
+        native.reset_stage_stats()
+        pix, dep = r.render(vp)
+        plain = shadow_launches()
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT, row_bands=1, shadow_queue_mb=1, profile_stages=True)
+        native.reset_stage_stats()
+        spix, sdep = r.render(vp, update_scene=False)
+        batched = shadow_launches()
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+    assert batched == 4 * plain                 # one light per batch
+    assert np.array_equal(spix, pix) and np.array_equal(sdep, dep)
+    opix, odep, _ = oracle_frame(w)
+    assert_pixels_close(spix, opix, w.width, w.height)
+    assert_depths_close(sdep, odep)
+    assert_float_pixels_close(spix, opix)

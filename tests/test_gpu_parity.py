@@ -116,6 +116,25 @@ def test_render_matches_oracle(name, engine):
 
 
 @pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("size", [(1, 1), (1, 7), (7, 1), (5, 3), (9, 5), (33, 17)])
+def test_tiny_and_ragged_canvases_match_oracle(size, engine):
+    """Canvases smaller than one 8x4 tile of primary numbering, one pixel wide
+    or high, and with partial tiles on both edges."""
+    native.set_render_options(engine=engine)
+    w = scenes.small_mesh_scene(0, *size)
+    r = renderer_for(w)
+    pix, dep = r.render(Viewport(w.camera, w.width, w.height))
+    opix, odep, _ = O.oracle_render(w.scene, w.projection(), w.settings, w.width, w.height, layout=L)
+    assert_pixels_close(pix, opix, w.width, w.height)
+    assert_depths_close(dep, odep)
+    g, p, d, b = gpu_primary(w.scene, w.projection(), w.width, w.height)
+    og, op, od, ob = O.oracle_trace_primary(w.scene, w.projection(), w.width, w.height)
+    assert np.array_equal(g, og) and np.array_equal(p, op)
+    assert np.array_equal(d.view(np.uint32), od.view(np.uint32))
+    native.set_render_options(engine=L.ENGINE_WAVEFRONT)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("mode", [L.RENDER_NORMALS, L.RENDER_DEPTH, L.RENDER_UVS, L.RENDER_MIP_LEVEL])
 def test_debug_modes(mode, engine):
     native.set_render_options(engine=engine)

@@ -1544,14 +1544,18 @@ cudaError_t trace_round(const RoundLaunch &L, QueueArgs &A, const CacheArgs &CA,
                                      dl->copy_stream)) != cudaSuccess)
                 return r;
         }
-        r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream);
-        if (r != cudaSuccess) return r;
+        // Scene arrays without meshes (split_extend is false exactly then)
+        // append no (shadow ray, instance) pairs: no pair counters, no mesh pass
+        // (config 3: 0.021 ms of a 0.56 ms whole-frame pass).
+        if (L.split_extend && (r = cudaMemsetAsync(B.queue_count + 3, 0, 2 * sizeof(uint32_t), stream)) != cudaSuccess)
+            return r;
         A.counters = L.stage(STAGE_SHADOW);
         if (timer) timer->begin(STAGE_SHADOW, stream);
         k_shadow_scene<COUNT, BATCH><<<L.grid((const void *)k_shadow_scene<COUNT, BATCH>, L.bound * (A.light_end - A.light_begin)),
                                       L.block, 0, stream>>>(S, F, A);
         count_launch();
         if (timer) timer->end(STAGE_SHADOW, stream);
+        if (!L.split_extend) continue;
         A.counters = L.stage(STAGE_SHADOW_MESH);
         if (timer) timer->begin(STAGE_SHADOW_MESH, stream);
         k_shadow_mesh<COUNT><<<L.mesh_grid((const void *)k_shadow_mesh<COUNT>, B.pair_capacity), kMeshBlock, 0,

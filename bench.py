@@ -49,7 +49,9 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
+    p.add_argument("--engine", default="auto", choices=["auto", "wavefront", "megakernel"],
+                   help="auto (the library's default): the fused kernel for frames of mesh-free scenes whose "
+                        "paths end at their first hit or that are small, the wavefront engine for the rest")
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--config", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
                    help="workload (default: config2, the metric's 1080p mesh PBR scene)")
@@ -852,7 +854,7 @@ def main():
     from slimtracincpp_b200 import native, scenes
     from slimtracincpp_b200.renderer import RayTracingRenderer, Viewport, make_canvas
 
-    engine = L.ENGINE_WAVEFRONT if args.engine == "wavefront" else L.ENGINE_MEGAKERNEL
+    engine = {"auto": L.ENGINE_AUTO, "wavefront": L.ENGINE_WAVEFRONT, "megakernel": L.ENGINE_MEGAKERNEL}[args.engine]
     w = scenes.CONFIGS[args.config](args.seed)
     lib = native.lib()
     st = w.settings
@@ -924,6 +926,7 @@ def main():
     native.reset_stage_stats()
     prof_ms = sum(timed_frames(torch, native, r, vp, sp, stream, [(d_pix, d_dep)] * args.steps, flush))
     stats = {s["name"]: s for s in native.stage_stats()}
+    engine_used = "megakernel" if stats.get("fused", {}).get("launches") else "wavefront"
 
     # end to end through the C ABI with host buffers
     native.set_render_options(engine=engine, row_bands=args.row_bands)
@@ -989,8 +992,8 @@ def main():
                        "max_depth": int(w.settings["max_depth"]), "geometries": len(w.scene.geometries),
                        "triangles": sum(m.triangle_count for m in w.scene.meshes),
                        "textures": len(w.scene.textures), "lights": len(w.scene.lights),
-                       "engine": args.engine, "parallelism": f"replicas x{world}",
-                       "row_bands": (args.row_bands or (2 if n >= 1 << 18 else 1)) if args.engine == "wavefront" else 1,
+                       "engine": args.engine, "engine_used": engine_used, "parallelism": f"replicas x{world}",
+                       "row_bands": (args.row_bands or (2 if n >= 1 << 18 else 1)) if engine_used == "wavefront" else 1,
                        "l2": "flushed between steps (512 MiB write)", "rays_per_frame": rays_per_frame,
                        "primary_rays": work["primary_rays"], "shadow_rays": work["shadow_rays"],
                        "bounce_rays": work["bounce_rays"]},
@@ -1008,7 +1011,7 @@ def main():
                                 "into a pinned canvas"},
             "clocks": clock_info,
             "gpu_launches": launches}
-    if args.config == "config2" and args.engine == "wavefront" and not args.no_cache_block:
+    if args.config == "config2" and engine_used == "wavefront" and not args.no_cache_block:
         # the metric's second half, in the same process: config 4 (this scene at
         # bounce depth 8), plain frames against radiance-cache frames
         w4 = scenes.config4(args.seed, meshes=w.scene.meshes)
@@ -1018,7 +1021,7 @@ def main():
         cmp["workload"] = w4.name
         cmp["nrc_roofline"] = nrc_roofline(torch, native, w4, dev)
         line["radiance_cache"] = cmp
-    if args.config == "config2" and args.engine == "wavefront" and not args.no_batch_block:
+    if args.config == "config2" and engine_used == "wavefront" and not args.no_batch_block:
         # config 5 (64 batched requests over config 2's meshes), same process
         line["batch"] = batch_comparison(torch, native, dev, min(args.steps, 5), min(args.warmup, 3), args.seed,
                                          meshes=w.scene.meshes)

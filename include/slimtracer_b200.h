@@ -181,11 +181,19 @@ typedef struct {                                              /* renderer/ray_tr
 } SlimRayTracerSettings;
 
 /* Options with no reference counterpart (B200 execution choices). */
-enum { SLIM_ENGINE_WAVEFRONT = 0, SLIM_ENGINE_MEGAKERNEL = 1 };
+enum { SLIM_ENGINE_WAVEFRONT = 0, SLIM_ENGINE_MEGAKERNEL = 1, SLIM_ENGINE_AUTO = 2 };
 enum { SLIM_CONES_REFERENCE = 0, SLIM_CONES_PER_PIXEL = 1 };
 enum { SLIM_SCENE_BVH_UPLOADED = 0, SLIM_SCENE_BVH_REFIT = 1 };
 typedef struct {
-    int32_t engine;          /* SLIM_ENGINE_*: wavefront queues (default) or one fused kernel */
+    int32_t engine;          /* SLIM_ENGINE_*: wavefront queues, one fused kernel, or AUTO --
+                                the library's setting until the first slimSetRenderOptions (a
+                                zeroed struct selects WAVEFRONT): the fused kernel for frames of
+                                scenes without meshes whose paths end at their first hit (max
+                                depth 1, or no reflective or refractive material) or that have
+                                fewer than 2^19 samples, the wavefront engine for the rest and
+                                for radiance-cache frames.  Both engines write the same pixels;
+                                the choice is speed only (fused: one launch, no queues; wavefront:
+                                split BVH walks that keep warps full on long or divergent paths) */
     int32_t ray_cones;       /* SLIM_CONES_REFERENCE (default): the reference's effective ray
                                 cone (mip 0: its copy of the aux hit clears the per-pixel
                                 spread); SLIM_CONES_PER_PIXEL: per-pixel spread */

@@ -150,6 +150,14 @@ struct PinnedBuffer {
     }
 };
 
+// The options a context starts with: every field zero, the engine chosen per
+// frame (SLIM_ENGINE_AUTO).
+SlimRenderOptions initial_options() {
+    SlimRenderOptions o{};
+    o.engine = SLIM_ENGINE_AUTO;
+    return o;
+}
+
 struct Context {
     bool initialized = false;
     int device = -1;
@@ -181,7 +189,7 @@ struct Context {
     uint32_t scene_node_count = 0;
 
     DevScene scene{};
-    SlimRenderOptions options{};
+    SlimRenderOptions options = initial_options();
     SlimWorkCounters last_counters{};
     // Queues of the wavefront engine: one set per band lane, so that many
     // row bands of a frame can be in flight at once (lane 0 on the caller's
@@ -751,6 +759,28 @@ int wait_for_refit(Context &c, cudaStream_t stream) {
     return SLIM_OK;
 }
 
+// Frames of fewer samples than this in scenes without meshes run the fused
+// kernel under SLIM_ENGINE_AUTO even when their paths bounce.  Measured on
+// one B200, render only, the fused kernel against the wavefront engine:
+// config 1's implicit scene (paths end at the first hit) 0.031 / 0.050 ms at
+// 320x180, 0.036 / 0.069 at 640x360, 0.105 / 0.129 at 1280x720, 0.209 /
+// 0.258 at 1920x1080; config 3's glass, mirror and texture scene at depth 8
+// 0.075 / 0.163, 0.109 / 0.192, 0.274 / 0.260, 0.506 / 0.449 ms.
+constexpr uint64_t kAutoFusedSamples = 1u << 19;
+
+// The engine a frame runs on: the option, or under SLIM_ENGINE_AUTO the
+// faster one for its scene and size (the pixels are the same).  Meshes and
+// radiance-cache frames need the wavefront engine's split walks and queues.
+int frame_engine(const Context &c, const SlimRayTracerSettings *settings, uint64_t samples) {
+    if (c.options.engine != SLIM_ENGINE_AUTO) return c.options.engine;
+    if (c.options.radiance_cache != SLIM_CACHE_OFF || c.scene.mesh_count) return SLIM_ENGINE_WAVEFRONT;
+    bool bounces = false;
+    if (settings->max_depth > 1)
+        for (const SlimMaterial &m : c.materials)
+            bounces |= (m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) != 0;
+    return !bounces || samples < kAutoFusedSamples ? SLIM_ENGINE_MEGAKERNEL : SLIM_ENGINE_WAVEFRONT;
+}
+
 // Renders the sample rows [row_begin, row_begin + rows) of the canvas (rows
 // 0: all of them); `first` clears the work counters (the first band of a
 // frame).
@@ -788,7 +818,7 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
                   "clear counters");
     StageTimer *timer = timer_for(c);
     cudaError_t e;
-    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) {
+    if (frame_engine(c, settings, (uint64_t)F.width * F.height) == SLIM_ENGINE_MEGAKERNEL) {
         e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer);
     } else {
         // the cache phase of a banded frame needs no path queues of its own
@@ -924,8 +954,8 @@ bool banded_cache(const Context &c) {
            k.config.train_samples && !c.options.count_work;
 }
 
-uint32_t row_bands(const Context &c, uint32_t sample_rows, uint32_t samples) {
-    if (c.options.engine == SLIM_ENGINE_MEGAKERNEL) return 1;
+uint32_t row_bands(const Context &c, const SlimRayTracerSettings *settings, uint32_t sample_rows, uint32_t samples) {
+    if (frame_engine(c, settings, samples) == SLIM_ENGINE_MEGAKERNEL) return 1;
     if (c.options.radiance_cache != SLIM_CACHE_OFF && !banded_cache(c)) return 1;
     uint32_t bands = c.options.row_bands ? (uint32_t)c.options.row_bands
                                          : (samples >= kMinBandedSamples ? kDefaultRowBands : 1u);
@@ -965,7 +995,7 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     uint32_t stride = dim.stride ? dim.stride : dim.width;
     const bool ssaa = canvas->antialias == SLIM_AA_SSAA;
     const uint32_t sample_rows = (uint32_t)dim.height * (ssaa ? 2 : 1);
-    const uint32_t bands = row_bands(c, sample_rows, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1));
+    const uint32_t bands = row_bands(c, settings, sample_rows, sample_rows * (uint32_t)dim.width * (ssaa ? 2 : 1));
     const bool download = host_pixels != nullptr;
     int rc;
     if (bands <= 1) {
@@ -991,7 +1021,8 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     // soon as its first round is done, and later pixels go straight there.
     float4 *mapped_pixels = nullptr;
     float *mapped_depths = nullptr;
-    const bool early = banded_download && c.options.engine == SLIM_ENGINE_WAVEFRONT &&
+    const bool early = banded_download &&
+                       frame_engine(c, settings, (uint64_t)sample_rows * dim.width * (ssaa ? 2 : 1)) == SLIM_ENGINE_WAVEFRONT &&
                        c.options.radiance_cache == SLIM_CACHE_OFF && settings->render_mode == SLIM_RENDER_BEAUTY &&
                        settings->max_depth >= 1 && mapped_host(host_pixels, (void **)&mapped_pixels) &&
                        mapped_host(host_depths, (void **)&mapped_depths);
@@ -1299,7 +1330,7 @@ int slimPick(const SlimCameraRayProjection *projection, int x, int y, SlimPick *
 int slimSetRenderOptions(const SlimRenderOptions *options) {
     std::lock_guard<std::mutex> lock(g_mutex);
     if (!options) return set_error(SLIM_ERR_ARGUMENT, "options is null");
-    if (options->engine < 0 || options->engine > 1 || options->ray_cones < 0 || options->ray_cones > 1 ||
+    if (options->engine < SLIM_ENGINE_WAVEFRONT || options->engine > SLIM_ENGINE_AUTO || options->ray_cones < 0 || options->ray_cones > 1 ||
         options->scene_bvh < 0 || options->scene_bvh > 1 || options->block_size < 0 || options->block_size > 256 ||
         (options->block_size % 32) || options->radiance_cache < SLIM_CACHE_OFF ||
         options->radiance_cache > SLIM_CACHE_EXACT || options->row_bands < 0 || options->row_bands > 64)

@@ -27,7 +27,7 @@ LIGHT_IS_SHADOWING = 2
 SCENE_HAD_EMISSIVE_QUADS = 1
 IMAGE_ALPHA, IMAGE_LINEAR, IMAGE_TILE, IMAGE_CHANNEL, IMAGE_MIPMAP, IMAGE_FLIP, IMAGE_WRAP, IMAGE_NORMAL, \
     IMAGE_CUBEMAP = (1 << i for i in range(9))
-ENGINE_WAVEFRONT, ENGINE_MEGAKERNEL = 0, 1
+ENGINE_WAVEFRONT, ENGINE_MEGAKERNEL, ENGINE_AUTO = 0, 1, 2
 CONES_REFERENCE, CONES_PER_PIXEL = 0, 1
 SCENE_BVH_UPLOADED, SCENE_BVH_REFIT = 0, 1
 

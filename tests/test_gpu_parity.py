@@ -378,3 +378,39 @@ def test_mesh_leaf_too_large_for_the_packed_record_is_refused():
     with pytest.raises(native.SlimError) as err:
         RayTracingRenderer(scene, max_depth=1)
     assert err.value.code == 4 and "64 triangles" in str(err.value)
+
+
+def _stage_launches(w, viewport):
+    native.reset_stage_stats()
+    pix, dep = renderer_for(w).render(viewport)
+    return pix, dep, {s["name"]: s["launches"] for s in native.stage_stats()}
+
+
+def test_auto_engine_picks_by_scene_and_size():
+    """SLIM_ENGINE_AUTO: the fused kernel for mesh-free frames whose paths end
+    at their first hit or that are small, the wavefront engine for mesh
+    scenes and for large frames whose paths bounce -- with the pixels both
+    explicit engines write, bit for bit, and the oracle's."""
+    cases = [
+        (scenes.config1(3, 320, 180), "fused"),                        # no meshes, no bounces
+        (scenes.small_textured_scene(2, 160, 90), "fused"),            # bounces, few samples
+        (scenes.config3(1, 1024, 512, tex_size=64, cube_size=32, irradiance_size=8), "extend"),  # bounces, 2^19 samples
+        (scenes.small_mesh_scene(1, 160, 90), "extend"),               # meshes
+    ]
+    try:
+        for w, stage in cases:
+            vp = Viewport(w.camera, w.width, w.height)
+            native.set_render_options(engine=L.ENGINE_AUTO, profile_stages=True)
+            pix, dep, launches = _stage_launches(w, vp)
+            other = "extend" if stage == "fused" else "fused"
+            assert launches.get(stage, 0) > 0 and launches.get(other, 0) == 0, (w.name, launches)
+            for engine in ENGINES:
+                native.set_render_options(engine=engine)
+                p2, d2 = renderer_for(w).render(vp)
+                assert np.array_equal(pix.view(np.uint32), p2.view(np.uint32)), (w.name, engine)
+                assert np.array_equal(dep.view(np.uint32), d2.view(np.uint32)), (w.name, engine)
+            opix, odep, _ = O.oracle_render(w.scene, w.projection(), w.settings, w.width, w.height, layout=L)
+            assert_pixels_close(pix, opix, w.width, w.height)
+            assert_depths_close(dep, odep)
+    finally:
+        native.set_render_options(engine=L.ENGINE_WAVEFRONT)

@@ -59,10 +59,12 @@ def test_cache_checkpoint_layout_and_refusals():
 
 def test_render_options_are_validated():
     """Options outside their ranges are refused without touching the device."""
-    for bad in ({"row_bands": -1}, {"row_bands": 65}, {"block_size": 48}, {"radiance_cache": 4}):
+    for bad in ({"row_bands": -1}, {"row_bands": 65}, {"block_size": 48}, {"radiance_cache": 4}, {"engine": 3},
+                {"engine": -1}):
         with pytest.raises(native.SlimError):
             native.set_render_options(**bad)
     native.set_render_options(row_bands=64)
+    native.set_render_options(engine=L.ENGINE_AUTO)
     native.set_render_options()
 
 

@@ -999,6 +999,16 @@ int render_frame(Context &c, const SlimCanvasData *canvas, const SlimCameraRayPr
     const bool download = host_pixels != nullptr;
     int rc;
     if (bands <= 1) {
+        // A fused frame into a pinned canvas the device can address: the
+        // kernel writes every pixel and depth once and reads none, so it
+        // writes them there, over PCIe while it renders, and no copy follows
+        // (config 1 end to end: 0.169 -> 0.141 ms).
+        float4 *mapped_pixels = nullptr;
+        float *mapped_depths = nullptr;
+        if (download &&
+            frame_engine(c, settings, (uint64_t)sample_rows * dim.width * (ssaa ? 2 : 1)) == SLIM_ENGINE_MEGAKERNEL &&
+            mapped_host(host_pixels, (void **)&mapped_pixels) && mapped_host(host_depths, (void **)&mapped_depths))
+            return render(c, canvas, projection, settings, mapped_pixels, mapped_depths, stream, 0, 0, true);
         if ((rc = render(c, canvas, projection, settings, d_pixels, d_depths, stream, 0, 0, true))) return rc;
         if (download) {
             SLIM_CUDA(cudaMemcpyAsync(host_pixels, d_pixels, pixel_count * sizeof(float4), cudaMemcpyDeviceToHost,

@@ -285,7 +285,8 @@ def test_banded_download_into_a_pinned_canvas(engine, antialias, scene):
     primary hits are shaded for shadow rays), and the pixels of later bounces
     are written into the host canvas directly: the canvas must equal the
     one-band frame bit for bit, for any band count (70 rows: the last band
-    also holds the rows past the last 4-row tile band)."""
+    also holds the rows past the last 4-row tile band).  The fused engine
+    writes a pinned canvas directly from its kernel, with no copy after it."""
     from slimtracincpp_b200.renderer import make_canvas
     w = BANDED_SCENES[scene]()
     r = renderer_for(w)

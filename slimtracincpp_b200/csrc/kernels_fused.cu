@@ -75,8 +75,11 @@ SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, ui
     out_depth = p.depth;
 }
 
+#ifndef SLIM_FUSED_MIN_BLOCKS
+#define SLIM_FUSED_MIN_BLOCKS 1
+#endif
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_render_fused(DevScene S, DevFrame F) {
+__global__ void __launch_bounds__(128, SLIM_FUSED_MIN_BLOCKS) k_render_fused(DevScene S, DevFrame F) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Work w = {};
     if (i < F.width * F.rows) {

@@ -771,14 +771,19 @@ constexpr uint64_t kAutoFusedSamples = 1u << 19;
 // The engine a frame runs on: the option, or under SLIM_ENGINE_AUTO the
 // faster one for its scene and size (the pixels are the same).  Meshes and
 // radiance-cache frames need the wavefront engine's split walks and queues.
+// Can a path of this frame go past its first hit?  Only through a
+// reflective or refractive material, with max depth above 1.
+bool paths_bounce(const Context &c, const SlimRayTracerSettings *settings) {
+    if (settings->max_depth <= 1) return false;
+    for (const SlimMaterial &m : c.materials)
+        if (m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) return true;
+    return false;
+}
+
 int frame_engine(const Context &c, const SlimRayTracerSettings *settings, uint64_t samples) {
     if (c.options.engine != SLIM_ENGINE_AUTO) return c.options.engine;
     if (c.options.radiance_cache != SLIM_CACHE_OFF || c.scene.mesh_count) return SLIM_ENGINE_WAVEFRONT;
-    bool bounces = false;
-    if (settings->max_depth > 1)
-        for (const SlimMaterial &m : c.materials)
-            bounces |= (m.flags & (SLIM_MATERIAL_IS_REFLECTIVE | SLIM_MATERIAL_IS_REFRACTIVE)) != 0;
-    return !bounces || samples < kAutoFusedSamples ? SLIM_ENGINE_MEGAKERNEL : SLIM_ENGINE_WAVEFRONT;
+    return !paths_bounce(c, settings) || samples < kAutoFusedSamples ? SLIM_ENGINE_MEGAKERNEL : SLIM_ENGINE_WAVEFRONT;
 }
 
 // Renders the sample rows [row_begin, row_begin + rows) of the canvas (rows
@@ -819,7 +824,7 @@ int render(Context &c, const SlimCanvasData *canvas, const SlimCameraRayProjecti
     StageTimer *timer = timer_for(c);
     cudaError_t e;
     if (frame_engine(c, settings, (uint64_t)F.width * F.height) == SLIM_ENGINE_MEGAKERNEL) {
-        e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer);
+        e = launch_render_fused(c.scene, F, c.options.block_size, stream, timer, !paths_bounce(c, settings));
     } else {
         // the cache phase of a banded frame needs no path queues of its own
         if (cache_part != kCachePartPhase && (rc = ensure_wavefront(c, F.width * F.rows, set))) return rc;

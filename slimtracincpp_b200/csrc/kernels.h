@@ -21,9 +21,11 @@ struct StageTimer {
     virtual ~StageTimer() = default;
 };
 
-// One thread per sample, the whole path in one kernel.
+// One thread per sample, the whole path in one kernel; `short_paths`: no
+// path can bounce (the build with more blocks per SM than the one for
+// bouncing paths).
 cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
-                                StageTimer *timer);
+                                StageTimer *timer, bool short_paths = false);
 
 // First closest hit of every primary ray.
 cudaError_t launch_trace_primary(const DevScene &S, const SlimCameraRayProjection &P, uint32_t width, uint32_t height,

@@ -75,11 +75,28 @@ SLIM_D void render_sample(const DevScene &S, const DevFrame &F, int x, int y, ui
     out_depth = p.depth;
 }
 
-#ifndef SLIM_FUSED_MIN_BLOCKS
-#define SLIM_FUSED_MIN_BLOCKS 1
+// Blocks per SM the fused kernel is compiled for (register caps with
+// spills that mostly hit L1), one build for frames whose paths end at their
+// first hit (no reflective or refractive material, or max depth 1) and one
+// for the rest.  Measured on one B200, frames without refit, blocks per SM
+// for short / long paths:
+//   4 / 4 (128 registers):  config 1 640x360 0.035 ms, 1920x1080 0.201;
+//                           config 3 (glass, depth 8) 320x180 0.075, 640x360 0.107
+//   5 / 4:                  config 1 0.039, 0.215
+//   6 / 4:                  config 1 0.041, 0.217
+//   4 / 3 (170 registers):  config 3 0.071, 0.107
+//   4 / 5:                  config 3 0.082, 0.123
+// (uncapped, 220 registers and two blocks: config 1 0.045 ms).
+#ifndef SLIM_FUSED_SHORT_BLOCKS
+#define SLIM_FUSED_SHORT_BLOCKS 4
 #endif
-template <bool COUNT>
-__global__ void __launch_bounds__(128, SLIM_FUSED_MIN_BLOCKS) k_render_fused(DevScene S, DevFrame F) {
+#ifndef SLIM_FUSED_LONG_BLOCKS
+#define SLIM_FUSED_LONG_BLOCKS 3
+#endif
+constexpr int kFusedShortPathBlocks = SLIM_FUSED_SHORT_BLOCKS;
+constexpr int kFusedLongPathBlocks = SLIM_FUSED_LONG_BLOCKS;
+template <bool COUNT, int MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MIN_BLOCKS) k_render_fused(DevScene S, DevFrame F) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     Work w = {};
     if (i < F.width * F.rows) {
@@ -246,19 +263,21 @@ cudaError_t launch_pick(const DevScene &S, const SlimCameraRayProjection &P, int
 }
 
 cudaError_t launch_render_fused(const DevScene &S, const DevFrame &F, int block, cudaStream_t stream,
-                                StageTimer *timer) {
+                                StageTimer *timer, bool short_paths) {
     uint32_t n = F.width * F.rows;
     if (block <= 0) block = 128;
     if (block > 128) block = 128;
     dim3 grid((n + block - 1) / block);
     if (timer) timer->begin(STAGE_FUSED, stream);
+    constexpr int kShort = dev::kFusedShortPathBlocks, kLong = dev::kFusedLongPathBlocks;
     if (F.counters) {
-        dev::k_render_fused<true><<<grid, block, 0, stream>>>(S, F);
-        count_launch();
+        if (short_paths) dev::k_render_fused<true, kShort><<<grid, block, 0, stream>>>(S, F);
+        else dev::k_render_fused<true, kLong><<<grid, block, 0, stream>>>(S, F);
     } else {
-        dev::k_render_fused<false><<<grid, block, 0, stream>>>(S, F);
-        count_launch();
+        if (short_paths) dev::k_render_fused<false, kShort><<<grid, block, 0, stream>>>(S, F);
+        else dev::k_render_fused<false, kLong><<<grid, block, 0, stream>>>(S, F);
     }
+    count_launch();
     if (timer) timer->end(STAGE_FUSED, stream);
     return cudaGetLastError();
 }
